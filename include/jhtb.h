@@ -1,0 +1,120 @@
+/*
+ * jhtb -- B200 (sm_100a) on-grid HEALPix spherical-harmonic transforms.
+ *
+ * Plain C ABI: opaque plan handle, device pointers, sizes, a CUDA stream passed
+ * as void*.  No C++ or torch types cross this boundary.  Every function returns
+ * an int status (JHTB_OK == 0); on failure jhtb_last_error() describes it.
+ * Nothing aborts or traps.
+ *
+ * Conventions (those of jht, src/jht/healpix.py:1-24):
+ *   - a_lm: healpy m-major packing, idx(l,m) = m(2 lmax + 1 - m)/2 + l, m >= 0 only,
+ *     K = (lmax+1)(lmax+2)/2 complex128 per component;
+ *   - orthonormal Y_lm with the Condon-Shortley phase, map = sum a_lm Y_lm;
+ *   - spin 2: components (E, B) <-> (Q, U), COSMO convention;
+ *   - maps: RING order, Npix = 12 nside^2 float64 per component.
+ * Batched layouts: alm [batch][ncomp][K] complex128, maps [batch][ncomp][Npix]
+ * float64, with ncomp = 1 (spin 0) or 2 (spin 2).
+ *
+ * Each entry point replaces one jht function (file:line in jht v0.2.0):
+ *   jhtb_plan_create        healpix.py:184-357  (_prepare: geometry, recursion plan, FFT plan)
+ *   jhtb_synthesis          healpix.py:363-387  (synthesis)
+ *   jhtb_adjoint_synthesis  healpix.py:390-412  (adjoint_synthesis)
+ *   jhtb_weighted_residual  _analysis.py:49-52, :58-60 (W * m and W * (m - S a))
+ *   jhtb_axpy               _analysis.py:60  (a + bare_analysis(...)), masked.py:313 (CG updates)
+ *   jhtb_dot                masked.py:313  (the inner products of the CG solve)
+ */
+#ifndef JHTB_H
+#define JHTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JHTB_OK 0
+#define JHTB_ERR_INVALID (-1)     /* bad argument (size, spin, precision, null pointer) */
+#define JHTB_ERR_UNSUPPORTED (-2) /* valid request the library does not implement */
+#define JHTB_ERR_CUDA (-3)        /* a CUDA runtime call failed */
+#define JHTB_ERR_NOMEM (-4)       /* device allocation failed */
+
+/* Arithmetic used by the contraction.  The recursion, seeds, coefficients and
+ * the ring FFTs are FP64 in every mode. */
+#define JHTB_PREC_FP64 0 /* plain FP64 everywhere */
+#define JHTB_PREC_FP32 1 /* FP32 contraction, FP32 accumulation */
+
+typedef struct jhtb_plan jhtb_plan;
+
+/* Optional host-computed seed inputs (host pointers; any member may be NULL, in
+ * which case the library computes it itself in FP64).  They let a caller hand
+ * over bit-identical copies of the tables its own reference implementation
+ * uses, e.g. jht's NumPy plan (_recursion.py:305-333):
+ *   x            [2 nside]   cos(theta) of the north-cap + equator rings
+ *   logsin       [2 nside]   log sin(theta)                (spin 0 seeds)
+ *   logcos_half  [2 nside]   log cos(theta/2)              (spin 2 seeds)
+ *   logsin_half  [2 nside]   log sin(theta/2)              (spin 2 seeds)
+ *   seed_logc    spin 0: [lmax+1] theta-independent log|lambda_mm|;
+ *                spin 2: [2][lmax+1] log-factor of d^{lmin}_{-m,+2}, then of d^{lmin}_{-m,-2} */
+typedef struct jhtb_host_tables {
+    const double *x;
+    const double *logsin;
+    const double *logcos_half;
+    const double *logsin_half;
+    const double *seed_logc;
+} jhtb_host_tables;
+
+/* Library version, e.g. 100 for 0.1.0. */
+int jhtb_version(void);
+
+/* Copy the calling thread's last error message into buf (NUL-terminated). */
+int jhtb_last_error(char *buf, size_t len);
+
+/* Build all geometry, recursion and FFT tables for (nside, lmax, spin) on the
+ * current CUDA device and allocate workspace for up to max_batch maps per
+ * launch (larger batches are processed in chunks).  spin must be 0 or 2;
+ * nside in [1, 4096]; lmax in [0, 16383].  tables may be NULL.
+ * Replaces healpix.py:184 _prepare. */
+int jhtb_plan_create(int nside, int lmax, int spin, int precision, int max_batch,
+                     const jhtb_host_tables *tables, jhtb_plan **out);
+
+/* Release every device allocation owned by the plan. */
+int jhtb_plan_destroy(jhtb_plan *plan);
+
+/* Device bytes held by the plan (tables + workspace). */
+int jhtb_plan_bytes(const jhtb_plan *plan, int64_t *bytes);
+
+/* Calls on one plan share its workspace: issue them in order on one stream (or
+ * synchronise between streams).  Different plans are independent. */
+
+/* S: alm (device, complex128 [batch][ncomp][K]) -> maps (device, float64
+ * [batch][ncomp][Npix]).  Stream-ordered on `stream` (a cudaStream_t, NULL =
+ * legacy default stream).  Inputs are not modified.  healpix.py:363-387. */
+int jhtb_synthesis(jhtb_plan *plan, const void *alm, void *maps, int batch, void *stream);
+
+/* S^T: maps (device float64) -> alm (device complex128), the exact transpose of
+ * jhtb_synthesis in the (2 - delta_m0)-weighted alm inner product.
+ * healpix.py:390-412. */
+int jhtb_adjoint_synthesis(jhtb_plan *plan, const void *maps, void *alm, int batch, void *stream);
+
+/* out[i] = w(pix i) * (maps[i] - synth[i]) for every component and map in the
+ * batch (synth may be NULL: out = w * maps).  w(pix) = (4 pi / Npix)(1 + ring_w[r'])
+ * with r' the north partner of the pixel's ring, or 4 pi / Npix when ring_w is NULL
+ * (weights.py:86-106).  ring_w: device float64 [2 nside]. */
+int jhtb_weighted_residual(const jhtb_plan *plan, const double *maps, const double *synth,
+                           const double *ring_w, double *out, int batch, void *stream);
+
+/* y[i] += alpha * x[i] over n float64 values (complex data: pass 2*count). */
+int jhtb_axpy(int64_t n, double alpha, const double *x, double *y, void *stream);
+
+/* *result (device float64) = sum_i x[i] y[i] over n values, FP64, fixed reduction
+ * order (bitwise reproducible).  Uses the plan's small reduction scratch, so calls
+ * on one plan must be ordered on one stream. */
+int jhtb_dot(const jhtb_plan *plan, int64_t n, const double *x, const double *y, double *result,
+             void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JHTB_H */

@@ -1,0 +1,113 @@
+// Internal definitions shared by the jhtb CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/jhtb.h"
+
+namespace jhtb {
+
+// ---------------------------------------------------------------------------------
+// error reporting (thread-local last error, int status codes; never abort)
+// ---------------------------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define JHTB_CUDA_TRY(expr)                                   \
+    do {                                                      \
+        cudaError_t _e = (expr);                              \
+        if (_e != cudaSuccess) return ::jhtb::cuda_fail(_e, #expr); \
+    } while (0)
+
+// ---------------------------------------------------------------------------------
+// scaled representation of the recursion: value = mant * 2^(800 * sc), sc <= 0.
+// While sc < 0 the value is far below any contribution that matters and is not
+// accumulated; when |mant| exceeds 2^400 it is rescaled by 2^-800 and sc steps up.
+// ---------------------------------------------------------------------------------
+constexpr double kBig = 0x1p400;
+constexpr double kScaleDown = 0x1p-800;
+constexpr double kLogScaleHi = 554.5177444475703;     // 800 ln 2, 41 significant bits
+constexpr double kLogScaleLo = 3.85953392016288e-10;  // 800 ln 2 - kLogScaleHi
+constexpr double kLn2x400 = 277.25887222397812;       // 400 ln 2
+
+// FFT: largest power-of-two length handled in one CTA's shared memory.
+constexpr int kFftMax = 8192;
+constexpr int kFftLogMax = 13;
+
+// Ring FFT modes.
+enum RingMode : int { kDirect = 0, kBluestein = 1 };
+
+struct RingDesc {
+    int N;          // pixels in the ring
+    int mode;       // kDirect (N a power of two <= kFftMax) or kBluestein
+    int P;          // FFT length: N (direct) or Bluestein length (power of two >= 2N-1)
+    int Q;          // number of kFftMax-point pieces for P > kFftMax (else 1)
+    long long start;   // first pixel
+    long long bh_off;  // offset (complex units) of this length's chirp spectrum
+    double phi0;       // azimuth of the first pixel
+};
+
+// Per-m seed parameters.  Spin 0: lf = theta-independent log|lambda_mm|,
+// sign = (-1)^m, pc = ps = 0.  Spin +-2: log|d^{lmin}_{-m,+-2}| = lf + pc log cos(t/2)
+// + ps log sin(t/2) with sign (_recursion.py:166-188).
+struct SeedParam {
+    double lf[2];
+    double sign[2];
+    int pc[2];
+    int ps[2];
+    int lmin;
+    int pad;
+};
+
+struct Plan {
+    int nside, lmax, spin, precision, max_batch;
+    int T;         // half-grid rings (north cap + equator) = 2 nside
+    int nrings;    // 4 nside - 1
+    int M;         // lmax + 1
+    long long K;   // packed alm size
+    long long npix;
+    int ncomp;     // 1 (spin 0) or 2 (spin 2)
+    int npairs;    // m-pairs (m, lmax - m)
+
+    // geometry (device)
+    double *d_x;        // [T] cos theta
+    double *d_logsin;   // [T] log sin theta       (spin 0 seeds)
+    double *d_logch;    // [T] log cos(theta/2)    (spin 2 seeds)
+    double *d_logsh;    // [T] log sin(theta/2)
+    RingDesc *d_rings;  // [nrings]
+    double2 *d_tw;      // [kFftMax] exp(-2 pi i k / kFftMax)
+    double2 *d_bh;      // Bluestein chirp spectra, FFT_P(conj(w))/P, per distinct length
+    long long bh_len;
+
+    // recursion tables (device), packed like the alm
+    SeedParam *d_seed;  // [M]
+    double *d_alpha;    // [K]
+    double *d_gamma;    // [K] (spin 2)
+    double *d_cnorm;    // [K]
+
+    // workspace
+    double2 *d_F;       // [chunk][nchan][nrings][M] ring spectra
+    double2 *d_W;       // [chunk][npix] Bluestein accumulation scratch (adjoint, Q > 1)
+    double *d_scratch;  // small reduction scratch
+    int chunk;          // maps per workspace pass
+    size_t bytes;
+};
+
+// kernels launchers (return 0 or a jhtb status)
+int launch_legendre_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaStream_t s);
+int launch_legendre_adjoint(const Plan &p, const double2 *F, double2 *alm, int nb, cudaStream_t s);
+int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cudaStream_t s);
+int launch_ring_adjoint(const Plan &p, const double *maps, double2 *F, double2 *W, int nb,
+                        cudaStream_t s);
+int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *offs, int nlen,
+                           cudaStream_t s);
+
+__host__ __device__ inline long long alm_index(long long l, long long m, long long lmax) {
+    return m * (2 * lmax + 1 - m) / 2 + l;
+}
+
+}  // namespace jhtb

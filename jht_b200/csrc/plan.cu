@@ -1,0 +1,379 @@
+// Plan construction and the C ABI entry points.
+//
+// A plan holds, on the device, everything that depends only on (nside, lmax,
+// spin): the RING geometry (jht healpix.py:107-140), per-m recursion seeds
+// (_recursion.py:53-56, :166-188), the normalised three-term recursion
+// coefficients, the per-ring FFT descriptors with Bluestein chirp spectra, and
+// the ring-spectrum workspace.  It replaces jht's lru-cached _prepare
+// (healpix.py:184-357), which builds the same information as NumPy constants.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "jhtb_internal.cuh"
+
+namespace jhtb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int code, const std::string &msg) {
+    set_error(msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    set_error(m);
+    return e == cudaErrorMemoryAllocation ? JHTB_ERR_NOMEM : JHTB_ERR_CUDA;
+}
+
+namespace {
+
+bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+long long next_pow2(long long n) {
+    long long p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// Compensated sum, for the theta-independent log of the sectoral seed.
+double kahan_log_const(int m) {
+    double s = -0.5 * std::log(4.0 * M_PI), c = 0.0;
+    for (int k = 1; k <= m; ++k) {
+        double y = 0.5 * std::log((2.0 * k + 1.0) / (2.0 * k)) - c;
+        double t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    return s;
+}
+
+// log|d^{lmin}_{M,M'}| constant, sign and the powers of cos(t/2), sin(t/2)
+// (_recursion.py:166-188).
+void wigner_seed_param(int M, int Mp, int lmin, double &lf, double &sign, int &pc, int &ps) {
+    int k0 = std::max(0, M - Mp);
+    lf = 0.5 * (std::lgamma(lmin + M + 1.0) + std::lgamma(lmin - M + 1.0) +
+                std::lgamma(lmin + Mp + 1.0) + std::lgamma(lmin - Mp + 1.0)) -
+         (std::lgamma(k0 + 1.0) + std::lgamma(lmin + M - k0 + 1.0) +
+          std::lgamma(lmin - Mp - k0 + 1.0) + std::lgamma(k0 - M + Mp + 1.0));
+    sign = (k0 % 2) ? -1.0 : 1.0;
+    pc = 2 * lmin - 2 * k0 + M - Mp;
+    ps = 2 * k0 - M + Mp;
+}
+
+template <typename T>
+int upload(T **dptr, const std::vector<T> &h, size_t &bytes) {
+    size_t n = h.size() * sizeof(T);
+    if (n == 0) n = sizeof(T);
+    JHTB_CUDA_TRY(cudaMalloc((void **)dptr, n));
+    bytes += n;
+    if (!h.empty()) JHTB_CUDA_TRY(cudaMemcpy(*dptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return JHTB_OK;
+}
+
+void free_plan(Plan *p) {
+    if (!p) return;
+    void *ptrs[] = {p->d_x,     p->d_logsin, p->d_logch, p->d_logsh,   p->d_rings, p->d_tw,
+                    p->d_bh,    p->d_seed,   p->d_alpha, p->d_gamma,   p->d_cnorm, p->d_F,
+                    p->d_W,     p->d_scratch};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    delete p;
+}
+
+int build_plan(Plan *p, const jhtb_host_tables *ht) {
+    const int nside = p->nside, L = p->lmax, spin = p->spin;
+    const int T = p->T, M = p->M, nr = p->nrings;
+    size_t &bytes = p->bytes;
+
+    // ---- RING geometry (healpix.py:107-140) -----------------------------------------
+    std::vector<double> z(nr), phi0(nr);
+    std::vector<long long> npr(nr), start(nr);
+    const double ns2 = 3.0 * (double)((long long)nside * nside);
+    for (int r = 0; r < nr; ++r) {
+        long long i = r + 1;
+        if (i < nside) {
+            npr[r] = 4 * i;
+            z[r] = 1.0 - (double)(i * i) / ns2;
+            phi0[r] = M_PI / (4.0 * (double)i);
+        } else if (i > 3LL * nside) {
+            long long ii = 4LL * nside - i;
+            npr[r] = 4 * ii;
+            z[r] = -(1.0 - (double)(ii * ii) / ns2);
+            phi0[r] = M_PI / (4.0 * (double)ii);
+        } else {
+            npr[r] = 4LL * nside;
+            z[r] = 4.0 / 3.0 - (2.0 * (double)i) / (3.0 * (double)nside);
+            phi0[r] = ((i - nside) % 2 == 0) ? M_PI / (4.0 * (double)nside) : 0.0;
+        }
+        start[r] = r == 0 ? 0 : start[r - 1] + npr[r - 1];
+    }
+
+    // ---- half-grid seed inputs ----------------------------------------------------------
+    std::vector<double> x(T), lsin(T), lch(T), lsh(T);
+    for (int t = 0; t < T; ++t) {
+        x[t] = ht && ht->x ? ht->x[t] : z[t];
+        double xx = x[t];
+        double s2 = std::min(std::max(1.0 - xx * xx, 0.0), 1.0);
+        double c2 = std::min(std::max((1.0 + xx) / 2.0, 0.0), 1.0);
+        double h2 = std::min(std::max((1.0 - xx) / 2.0, 0.0), 1.0);
+        lsin[t] = ht && ht->logsin ? ht->logsin[t] : std::log(std::sqrt(s2));
+        lch[t] = ht && ht->logcos_half ? ht->logcos_half[t] : std::log(std::sqrt(c2));
+        lsh[t] = ht && ht->logsin_half ? ht->logsin_half[t] : std::log(std::sqrt(h2));
+    }
+    int rc;
+    if ((rc = upload(&p->d_x, x, bytes))) return rc;
+    if ((rc = upload(&p->d_logsin, lsin, bytes))) return rc;
+    if ((rc = upload(&p->d_logch, lch, bytes))) return rc;
+    if ((rc = upload(&p->d_logsh, lsh, bytes))) return rc;
+
+    // ---- per-m seeds ---------------------------------------------------------------------
+    std::vector<SeedParam> seeds(M);
+    for (int m = 0; m < M; ++m) {
+        SeedParam &sp = seeds[m];
+        std::memset(&sp, 0, sizeof(sp));
+        if (spin == 0) {
+            sp.lmin = m;
+            sp.lf[0] = ht && ht->seed_logc ? ht->seed_logc[m] : kahan_log_const(m);
+            sp.sign[0] = (m % 2) ? -1.0 : 1.0;
+        } else {
+            sp.lmin = std::max(m, 2);
+            for (int h = 0; h < 2; ++h) {
+                int s = h == 0 ? 2 : -2;
+                wigner_seed_param(-m, s, sp.lmin, sp.lf[h], sp.sign[h], sp.pc[h], sp.ps[h]);
+                if (ht && ht->seed_logc) sp.lf[h] = ht->seed_logc[h * M + m];
+            }
+        }
+    }
+    if ((rc = upload(&p->d_seed, seeds, bytes))) return rc;
+
+    // ---- normalised recursion coefficients ------------------------------------------------
+    // y_l = (P_l x + Q_l) y_{l-1} - R_l y_{l-2} with y = lambda / f (f = 1 for spin 0,
+    // (-1)^m sqrt((2l+1)/4pi) for spin 2).  Writing y_l = g_l mu_l with g_lmin = g_lmin+1 = 1,
+    // g_l = R_l g_{l-2}, gives mu_l = (alpha_l x + gamma_l) mu_{l-1} - mu_{l-2} and
+    // lambda_l = c_l mu_l, c_l = f_l g_l.  alpha = gamma = 0 at l = lmin (the seed step).
+    const long long K = p->K;
+    std::vector<double> alpha(K, 0.0), gamma(spin ? K : 0, 0.0), cnorm(K, 0.0);
+    for (int m = 0; m <= L; ++m) {
+        const int lmin = seeds[m].lmin;
+        double g2 = 1.0, g1 = 1.0;  // g_{l-2}, g_{l-1}
+        const double fsign = (spin && (m % 2)) ? -1.0 : 1.0;
+        for (int l = lmin; l <= L; ++l) {
+            const long long idx = alm_index(l, m, L);
+            double P = 0, Q = 0, R = 0;
+            if (l > lmin) {
+                if (spin == 0) {
+                    double dl = l;
+                    P = std::sqrt((2 * dl - 1) * (2 * dl + 1) / ((dl - m) * (dl + m)));
+                    R = std::sqrt((2 * dl + 1) * ((dl - 1) * (dl - 1) - (double)m * m) /
+                                  ((2 * dl - 3) * (dl - m) * (dl + m)));
+                } else {
+                    // Wigner-d coefficients at l-1 producing d^l (_recursion.py:136-143)
+                    double Lp = l - 1, Mm = -m, Mp = 2;
+                    double D = Lp * std::sqrt(((Lp + 1) * (Lp + 1) - Mm * Mm) * ((Lp + 1) * (Lp + 1) - Mp * Mp));
+                    P = (2 * Lp + 1) * Lp * (Lp + 1) / D;
+                    Q = -(2 * Lp + 1) * Mm * Mp / D;
+                    R = (Lp + 1) * std::sqrt((Lp * Lp - Mm * Mm) * (Lp * Lp - Mp * Mp)) / D;
+                }
+            }
+            double g;
+            if (l <= lmin + 1) g = 1.0;
+            else g = R * g2;
+            if (l > lmin) {
+                alpha[idx] = P * g1 / g;
+                if (spin) gamma[idx] = Q * g1 / g;
+            }
+            const double f = spin ? fsign * std::sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) : 1.0;
+            cnorm[idx] = f * g;
+            if (l > lmin) { g2 = g1; g1 = g; } else { g2 = 1.0; g1 = 1.0; }
+        }
+    }
+    if ((rc = upload(&p->d_alpha, alpha, bytes))) return rc;
+    if (spin && (rc = upload(&p->d_gamma, gamma, bytes))) return rc;
+    if ((rc = upload(&p->d_cnorm, cnorm, bytes))) return rc;
+
+    // ---- ring FFT descriptors -------------------------------------------------------------
+    std::vector<RingDesc> rings(nr);
+    std::map<long long, long long> bh_offset;  // Bluestein length -> offset
+    std::vector<int> blens;
+    std::vector<long long> boffs;
+    long long bh_len = 0;
+    for (int r = 0; r < nr; ++r) {
+        RingDesc &d = rings[r];
+        d.N = (int)npr[r];
+        d.start = start[r];
+        d.phi0 = phi0[r];
+        if (is_pow2(d.N) && d.N <= kFftMax) {
+            d.mode = kDirect;
+            d.P = d.N;
+            d.Q = 1;
+            d.bh_off = 0;
+        } else {
+            d.mode = kBluestein;
+            d.P = (int)next_pow2(2LL * d.N - 1);
+            d.Q = std::max(1, d.P / kFftMax);
+            if (d.Q > 4) return fail(JHTB_ERR_UNSUPPORTED, "ring length too large (nside > 4096)");
+            auto it = bh_offset.find(d.N);
+            if (it == bh_offset.end()) {
+                bh_offset[d.N] = bh_len;
+                blens.push_back(d.N);
+                boffs.push_back(bh_len);
+                d.bh_off = bh_len;
+                bh_len += d.P;
+            } else {
+                d.bh_off = it->second;
+            }
+        }
+    }
+    if ((rc = upload(&p->d_rings, rings, bytes))) return rc;
+
+    std::vector<double2> tw(kFftMax);
+    for (int k = 0; k < kFftMax; ++k) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)kFftMax;
+        tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    if ((rc = upload(&p->d_tw, tw, bytes))) return rc;
+
+    p->bh_len = bh_len;
+    JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_bh, sizeof(double2) * std::max(bh_len, 1LL)));
+    bytes += sizeof(double2) * std::max(bh_len, 1LL);
+
+    // ---- workspace --------------------------------------------------------------------------
+    const size_t f_per_map = sizeof(double2) * (size_t)p->ncomp * nr * M;
+    p->chunk = std::max(1, p->max_batch);
+    JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_F, f_per_map * p->chunk));
+    bytes += f_per_map * p->chunk;
+    bool need_w = false;
+    for (auto &d : rings) need_w |= (d.mode == kBluestein);
+    if (need_w) {
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_W, sizeof(double2) * (size_t)p->npix * p->chunk));
+        bytes += sizeof(double2) * (size_t)p->npix * p->chunk;
+    }
+    JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_scratch, 4096 * sizeof(double)));
+    bytes += 4096 * sizeof(double);
+
+    // ---- Bluestein chirp spectra (device) -------------------------------------------------------
+    if (!blens.empty()) {
+        int *d_len = nullptr;
+        long long *d_off = nullptr;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&d_len, sizeof(int) * blens.size()));
+        JHTB_CUDA_TRY(cudaMalloc((void **)&d_off, sizeof(long long) * boffs.size()));
+        JHTB_CUDA_TRY(cudaMemcpy(d_len, blens.data(), sizeof(int) * blens.size(), cudaMemcpyHostToDevice));
+        JHTB_CUDA_TRY(cudaMemcpy(d_off, boffs.data(), sizeof(long long) * boffs.size(), cudaMemcpyHostToDevice));
+        rc = launch_bluestein_setup(*p, d_len, d_off, (int)blens.size(), 0);
+        cudaError_t e = cudaDeviceSynchronize();
+        cudaFree(d_len);
+        cudaFree(d_off);
+        if (rc) return rc;
+        if (e != cudaSuccess) return cuda_fail(e, "bluestein setup");
+    }
+    return JHTB_OK;
+}
+
+}  // namespace
+}  // namespace jhtb
+
+using namespace jhtb;
+
+extern "C" {
+
+int jhtb_version(void) { return 100; }
+
+int jhtb_last_error(char *buf, size_t len) {
+    if (!buf || len == 0) return JHTB_ERR_INVALID;
+    std::snprintf(buf, len, "%s", g_last_error.c_str());
+    return JHTB_OK;
+}
+
+int jhtb_plan_create(int nside, int lmax, int spin, int precision, int max_batch,
+                     const jhtb_host_tables *tables, jhtb_plan **out) {
+    if (!out) return fail(JHTB_ERR_INVALID, "jhtb_plan_create: out is NULL");
+    *out = nullptr;
+    if (spin != 0 && spin != 2)
+        return fail(JHTB_ERR_UNSUPPORTED, "spin=" + std::to_string(spin) + " unsupported (only 0 and 2)");
+    if (nside < 1 || nside > 4096)
+        return fail(JHTB_ERR_INVALID, "nside must be in [1, 4096], got " + std::to_string(nside));
+    if (lmax < 0 || lmax > 16383) return fail(JHTB_ERR_INVALID, "lmax must be in [0, 16383]");
+    if (precision != JHTB_PREC_FP64 && precision != JHTB_PREC_FP32)
+        return fail(JHTB_ERR_INVALID, "unknown precision " + std::to_string(precision));
+    if (max_batch < 1) return fail(JHTB_ERR_INVALID, "max_batch must be >= 1");
+    Plan *p = new (std::nothrow) Plan();
+    if (!p) return fail(JHTB_ERR_NOMEM, "host allocation failed");
+    std::memset(p, 0, sizeof(Plan));
+    p->nside = nside;
+    p->lmax = lmax;
+    p->spin = spin;
+    p->precision = precision;
+    p->max_batch = max_batch;
+    p->T = 2 * nside;
+    p->nrings = 4 * nside - 1;
+    p->M = lmax + 1;
+    p->K = (long long)(lmax + 1) * (lmax + 2) / 2;
+    p->npix = 12LL * nside * nside;
+    p->ncomp = spin ? 2 : 1;
+    p->npairs = lmax / 2 + 1;
+    int rc = build_plan(p, tables);
+    if (rc) {
+        free_plan(p);
+        return rc;
+    }
+    *out = reinterpret_cast<jhtb_plan *>(p);
+    return JHTB_OK;
+}
+
+int jhtb_plan_destroy(jhtb_plan *plan) {
+    free_plan(reinterpret_cast<Plan *>(plan));
+    return JHTB_OK;
+}
+
+int jhtb_plan_bytes(const jhtb_plan *plan, int64_t *bytes) {
+    if (!plan || !bytes) return fail(JHTB_ERR_INVALID, "jhtb_plan_bytes: NULL argument");
+    *bytes = (int64_t) reinterpret_cast<const Plan *>(plan)->bytes;
+    return JHTB_OK;
+}
+
+int jhtb_synthesis(jhtb_plan *plan, const void *alm, void *maps, int batch, void *stream) {
+    if (!plan || !alm || !maps) return fail(JHTB_ERR_INVALID, "jhtb_synthesis: NULL argument");
+    if (batch < 0) return fail(JHTB_ERR_INVALID, "jhtb_synthesis: negative batch");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    cudaStream_t s = (cudaStream_t)stream;
+    const double2 *a = (const double2 *)alm;
+    double *m = (double *)maps;
+    for (int b0 = 0; b0 < batch; b0 += p.chunk) {
+        int nb = std::min(p.chunk, batch - b0);
+        int rc = launch_legendre_synth(p, a + (size_t)b0 * p.ncomp * p.K, p.d_F, nb, s);
+        if (rc) return rc;
+        rc = launch_ring_synth(p, p.d_F, m + (size_t)b0 * p.ncomp * p.npix, nb, s);
+        if (rc) return rc;
+    }
+    return JHTB_OK;
+}
+
+int jhtb_adjoint_synthesis(jhtb_plan *plan, const void *maps, void *alm, int batch, void *stream) {
+    if (!plan || !alm || !maps) return fail(JHTB_ERR_INVALID, "jhtb_adjoint_synthesis: NULL argument");
+    if (batch < 0) return fail(JHTB_ERR_INVALID, "jhtb_adjoint_synthesis: negative batch");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    cudaStream_t s = (cudaStream_t)stream;
+    const double *m = (const double *)maps;
+    double2 *a = (double2 *)alm;
+    for (int b0 = 0; b0 < batch; b0 += p.chunk) {
+        int nb = std::min(p.chunk, batch - b0);
+        int rc = launch_ring_adjoint(p, m + (size_t)b0 * p.ncomp * p.npix, p.d_F, p.d_W, nb, s);
+        if (rc) return rc;
+        rc = launch_legendre_adjoint(p, p.d_F, a + (size_t)b0 * p.ncomp * p.K, nb, s);
+        if (rc) return rc;
+    }
+    return JHTB_OK;
+}
+
+}  // extern "C"
