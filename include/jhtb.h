@@ -113,6 +113,29 @@ int jhtb_axpy(int64_t n, double alpha, const double *x, double *y, void *stream)
 int jhtb_dot(const jhtb_plan *plan, int64_t n, const double *x, const double *y, double *result,
              void *stream);
 
+/* ---- diagnostics (no counterpart in jht; its profiling is by stage-timing scripts,
+ * scripts/profile_adjoint.py) ---------------------------------------------------- */
+
+/* Stages reported by jhtb_plan_timings. */
+#define JHTB_STAGE_LEGENDRE_SYNTH 0 /* fused recursion + contraction, synthesis   */
+#define JHTB_STAGE_RING_SYNTH 1     /* phase, fold and inverse ring DFTs           */
+#define JHTB_STAGE_RING_ADJOINT 2   /* forward ring DFTs, gather and phase         */
+#define JHTB_STAGE_LEGENDRE_ADJOINT 3 /* fused recursion + contraction, adjoint    */
+
+/* When enabled, every stage launch of this plan is bracketed by CUDA events on its
+ * stream.  Adds no synchronisation. */
+int jhtb_plan_set_timing(jhtb_plan *plan, int enable);
+
+/* Sum of recorded stage times (ms[4], milliseconds) and launch counts (counts[4]);
+ * waits for the recorded events.  reset != 0 drops the records. */
+int jhtb_plan_timings(jhtb_plan *plan, double *ms, int64_t *counts, int reset);
+
+/* FP64 FMA throughput probe: a grid of 148*blocks_per_sm CTAs x 256 threads, each
+ * running 8 independent FMA chains for `iters` steps.  Writes the elapsed time of
+ * the launch (CUDA events on `stream`) to *ms and the FLOP count (2 per FMA) to
+ * *flops; sink (device, >= 1 double) keeps the result live. */
+int jhtb_probe_fp64_fma(int blocks_per_sm, int iters, double *sink, double *ms, double *flops, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,6 +37,9 @@ EXPORTS = (
     "jhtb_weighted_residual",
     "jhtb_axpy",
     "jhtb_dot",
+    "jhtb_plan_set_timing",
+    "jhtb_plan_timings",
+    "jhtb_probe_fp64_fma",
 )
 
 
@@ -83,6 +86,10 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_weighted_residual": (i32, [vp, dp, dp, dp, dp, i32, vp]),
             "jhtb_axpy": (i32, [i64, ctypes.c_double, dp, dp, vp]),
             "jhtb_dot": (i32, [vp, i64, dp, dp, dp, vp]),
+            "jhtb_plan_set_timing": (i32, [vp, i32]),
+            "jhtb_plan_timings": (i32, [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64), i32]),
+            "jhtb_probe_fp64_fma": (i32, [i32, i32, dp, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_double), vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -185,6 +192,17 @@ class Plan:
         b = ctypes.c_int64()
         check(self.lib.jhtb_plan_bytes(self.handle, ctypes.byref(b)), "jhtb_plan_bytes")
         return int(b.value)
+
+    def set_timing(self, enable: bool) -> None:
+        check(self.lib.jhtb_plan_set_timing(self.handle, int(enable)), "jhtb_plan_set_timing")
+
+    def timings(self, reset: bool = True) -> dict[str, tuple[float, int]]:
+        """Per-stage (total ms, launches) since the last reset."""
+        ms = (ctypes.c_double * 4)()
+        cnt = (ctypes.c_int64 * 4)()
+        check(self.lib.jhtb_plan_timings(self.handle, ms, cnt, int(reset)), "jhtb_plan_timings")
+        names = ("legendre_synth", "ring_synth", "ring_adjoint", "legendre_adjoint")
+        return {n: (float(ms[i]), int(cnt[i])) for i, n in enumerate(names)}
 
     def close(self) -> None:
         if getattr(self, "handle", None):

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/jhtb.h"
 
@@ -95,7 +96,17 @@ struct Plan {
     double *d_scratch;  // small reduction scratch
     int chunk;          // maps per workspace pass
     size_t bytes;
+
+    // optional per-stage timing (CUDA events recorded on the launch stream)
+    bool timing;
+    struct StageEvent {
+        cudaEvent_t start, stop;
+        int stage;
+    };
+    std::vector<StageEvent> events;
 };
+
+enum Stage : int { kStageLegSynth = 0, kStageRingSynth = 1, kStageRingAdj = 2, kStageLegAdj = 3, kNumStages = 4 };
 
 // kernels launchers (return 0 or a jhtb status)
 int launch_legendre_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaStream_t s);

@@ -88,6 +88,10 @@ void free_plan(Plan *p) {
                     p->d_W,     p->d_scratch};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    for (auto &e : p->events) {
+        cudaEventDestroy(e.start);
+        cudaEventDestroy(e.stop);
+    }
     delete p;
 }
 
@@ -281,6 +285,29 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
 }
 
 }  // namespace
+
+// Records an event pair around one stage launch when the plan's timing is on.
+struct StageTimer {
+    Plan &p;
+    cudaStream_t s;
+    Plan::StageEvent ev{};
+    bool on;
+    StageTimer(Plan &plan, cudaStream_t stream, int stage) : p(plan), s(stream), on(plan.timing) {
+        if (!on) return;
+        ev.stage = stage;
+        if (cudaEventCreate(&ev.start) != cudaSuccess || cudaEventCreate(&ev.stop) != cudaSuccess) {
+            on = false;
+            return;
+        }
+        cudaEventRecord(ev.start, s);
+    }
+    ~StageTimer() {
+        if (!on) return;
+        cudaEventRecord(ev.stop, s);
+        p.events.push_back(ev);
+    }
+};
+
 }  // namespace jhtb
 
 using namespace jhtb;
@@ -304,12 +331,13 @@ int jhtb_plan_create(int nside, int lmax, int spin, int precision, int max_batch
     if (nside < 1 || nside > 4096)
         return fail(JHTB_ERR_INVALID, "nside must be in [1, 4096], got " + std::to_string(nside));
     if (lmax < 0 || lmax > 16383) return fail(JHTB_ERR_INVALID, "lmax must be in [0, 16383]");
-    if (precision != JHTB_PREC_FP64 && precision != JHTB_PREC_FP32)
+    if (precision == JHTB_PREC_FP32)
+        return fail(JHTB_ERR_UNSUPPORTED, "FP32 contraction is not available in this build");
+    if (precision != JHTB_PREC_FP64)
         return fail(JHTB_ERR_INVALID, "unknown precision " + std::to_string(precision));
     if (max_batch < 1) return fail(JHTB_ERR_INVALID, "max_batch must be >= 1");
-    Plan *p = new (std::nothrow) Plan();
+    Plan *p = new (std::nothrow) Plan();  // value-initialised: pointers null, counters zero
     if (!p) return fail(JHTB_ERR_NOMEM, "host allocation failed");
-    std::memset(p, 0, sizeof(Plan));
     p->nside = nside;
     p->lmax = lmax;
     p->spin = spin;
@@ -351,9 +379,16 @@ int jhtb_synthesis(jhtb_plan *plan, const void *alm, void *maps, int batch, void
     double *m = (double *)maps;
     for (int b0 = 0; b0 < batch; b0 += p.chunk) {
         int nb = std::min(p.chunk, batch - b0);
-        int rc = launch_legendre_synth(p, a + (size_t)b0 * p.ncomp * p.K, p.d_F, nb, s);
+        int rc;
+        {
+            StageTimer t(p, s, kStageLegSynth);
+            rc = launch_legendre_synth(p, a + (size_t)b0 * p.ncomp * p.K, p.d_F, nb, s);
+        }
         if (rc) return rc;
-        rc = launch_ring_synth(p, p.d_F, m + (size_t)b0 * p.ncomp * p.npix, nb, s);
+        {
+            StageTimer t(p, s, kStageRingSynth);
+            rc = launch_ring_synth(p, p.d_F, m + (size_t)b0 * p.ncomp * p.npix, nb, s);
+        }
         if (rc) return rc;
     }
     return JHTB_OK;
@@ -368,10 +403,47 @@ int jhtb_adjoint_synthesis(jhtb_plan *plan, const void *maps, void *alm, int bat
     double2 *a = (double2 *)alm;
     for (int b0 = 0; b0 < batch; b0 += p.chunk) {
         int nb = std::min(p.chunk, batch - b0);
-        int rc = launch_ring_adjoint(p, m + (size_t)b0 * p.ncomp * p.npix, p.d_F, p.d_W, nb, s);
+        int rc;
+        {
+            StageTimer t(p, s, kStageRingAdj);
+            rc = launch_ring_adjoint(p, m + (size_t)b0 * p.ncomp * p.npix, p.d_F, p.d_W, nb, s);
+        }
         if (rc) return rc;
-        rc = launch_legendre_adjoint(p, p.d_F, a + (size_t)b0 * p.ncomp * p.K, nb, s);
+        {
+            StageTimer t(p, s, kStageLegAdj);
+            rc = launch_legendre_adjoint(p, p.d_F, a + (size_t)b0 * p.ncomp * p.K, nb, s);
+        }
         if (rc) return rc;
+    }
+    return JHTB_OK;
+}
+
+int jhtb_plan_set_timing(jhtb_plan *plan, int enable) {
+    if (!plan) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_timing: NULL plan");
+    reinterpret_cast<Plan *>(plan)->timing = enable != 0;
+    return JHTB_OK;
+}
+
+int jhtb_plan_timings(jhtb_plan *plan, double *ms, int64_t *counts, int reset) {
+    if (!plan || !ms || !counts) return fail(JHTB_ERR_INVALID, "jhtb_plan_timings: NULL argument");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    for (int i = 0; i < kNumStages; ++i) {
+        ms[i] = 0.0;
+        counts[i] = 0;
+    }
+    for (auto &e : p.events) {
+        JHTB_CUDA_TRY(cudaEventSynchronize(e.stop));
+        float t = 0.f;
+        JHTB_CUDA_TRY(cudaEventElapsedTime(&t, e.start, e.stop));
+        ms[e.stage] += t;
+        counts[e.stage] += 1;
+    }
+    if (reset) {
+        for (auto &e : p.events) {
+            cudaEventDestroy(e.start);
+            cudaEventDestroy(e.stop);
+        }
+        p.events.clear();
     }
     return JHTB_OK;
 }

@@ -132,3 +132,51 @@ int jhtb_dot(const jhtb_plan *plan, int64_t n, const double *x, const double *y,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// FP64 FMA throughput probe (the denominator of the FP64 roofline fraction)
+// ---------------------------------------------------------------------------------------
+namespace jhtb {
+namespace {
+__global__ void __launch_bounds__(256) fp64_fma_probe_kernel(int iters, double *sink) {
+    double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-10, a2 = a0 + 2e-10, a3 = a0 + 3e-10;
+    double a4 = a0 + 4e-10, a5 = a0 + 5e-10, a6 = a0 + 6e-10, a7 = a0 + 7e-10;
+    const double b = 0.999999999, c = 1e-12;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+            a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+        }
+    }
+    const double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 12345.6789) sink[0] = s;  // never true; keeps the chains live
+}
+}  // namespace
+}  // namespace jhtb
+
+extern "C" int jhtb_probe_fp64_fma(int blocks_per_sm, int iters, double *sink, double *ms, double *flops,
+                                   void *stream) {
+    using namespace jhtb;
+    if (blocks_per_sm < 1 || iters < 1 || !sink || !ms || !flops) return fail(JHTB_ERR_INVALID, "jhtb_probe_fp64_fma: bad argument");
+    int dev = 0, nsm = 148;
+    JHTB_CUDA_TRY(cudaGetDevice(&dev));
+    JHTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    JHTB_CUDA_TRY(cudaEventCreate(&e0));
+    JHTB_CUDA_TRY(cudaEventCreate(&e1));
+    const int grid = nsm * blocks_per_sm;
+    JHTB_CUDA_TRY(cudaEventRecord(e0, s));
+    fp64_fma_probe_kernel<<<grid, 256, 0, s>>>(iters, sink);
+    JHTB_CUDA_TRY(cudaGetLastError());
+    JHTB_CUDA_TRY(cudaEventRecord(e1, s));
+    JHTB_CUDA_TRY(cudaEventSynchronize(e1));
+    float t = 0.f;
+    JHTB_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t;
+    *flops = 2.0 * 8.0 * 16.0 * (double)iters * 256.0 * (double)grid;
+    return JHTB_OK;
+}
