@@ -113,6 +113,17 @@ int jhtb_axpy(int64_t n, double alpha, const double *x, double *y, void *stream)
 int jhtb_dot(const jhtb_plan *plan, int64_t n, const double *x, const double *y, double *result,
              void *stream);
 
+/* Spin-0 FP64 synthesis that allocates nothing, for callers that cannot call
+ * cudaMalloc (a host framework or plugin that owns every device allocation, or a
+ * process whose device memory is already reserved).  No counterpart in jht.
+ * alm: device complex128 [K]; map: device float64 [12 nside^2].  Needs no plan:
+ * its only scratch is a fixed 2 MiB __device__ array inside the library, which
+ * limits it to nside <= 64, lmax <= 1023 and (4 nside - 1)(lmax + 1) <= 131072
+ * (larger sizes are rejected with JHTB_ERR_INVALID).  All calls share that array:
+ * calls that overlap on the GPU race, so order them on one stream.  The first call
+ * on each device looks up the array's address; make it before any stream capture. */
+int jhtb_synthesis_noalloc(int nside, int lmax, const void *alm, void *map, void *stream);
+
 /* ---- diagnostics (no counterpart in jht; its profiling is by stage-timing scripts,
  * scripts/profile_adjoint.py) ---------------------------------------------------- */
 

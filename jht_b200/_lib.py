@@ -40,6 +40,7 @@ EXPORTS = (
     "jhtb_plan_set_timing",
     "jhtb_plan_timings",
     "jhtb_probe_fp64_fma",
+    "jhtb_synthesis_noalloc",
 )
 
 
@@ -90,6 +91,7 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_plan_timings": (i32, [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64), i32]),
             "jhtb_probe_fp64_fma": (i32, [i32, i32, dp, ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double), vp]),
+            "jhtb_synthesis_noalloc": (i32, [i32, i32, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
