@@ -35,6 +35,10 @@ constexpr double kLogScaleHi = 554.5177444475703;     // 800 ln 2, 41 significan
 constexpr double kLogScaleLo = 3.85953392016288e-10;  // 800 ln 2 - kLogScaleHi
 constexpr double kLn2x400 = 277.25887222397812;       // 400 ln 2
 
+// Legendre kernels: half-grid rings per lane (a warp tile is 32 * R consecutive rings).
+constexpr int kR0 = 4;  // spin 0
+constexpr int kR2 = 2;  // spin 2
+
 // FFT: largest power-of-two length handled in one CTA's shared memory.
 constexpr int kFftMax = 8192;
 constexpr int kFftLogMax = 13;
@@ -90,6 +94,19 @@ struct Plan {
     double *d_gamma;    // [K] (spin 2)
     double *d_cnorm;    // [K]
 
+    // Legendre work items (plan creation): start l and recursion state per (m, warp tile),
+    // cost-sorted item orders for the persistent kernels
+    int ntiles;          // warp tiles per m
+    int nsuper, tps;     // adjoint: ring quarters per m, warp tiles per quarter
+    int *d_lw;           // [M * ntiles]
+    double2 *d_st;       // [M * ntiles][nrec][R][32]
+    int *d_stsc;         // [M * ntiles][nrec][R][32]
+    int *d_synth_order;  // [M * ntiles]
+    int *d_adj_order;    // [M * nsuper]
+    int *d_adj_tiles;    // [M * nsuper][tps]
+    unsigned *d_counter; // work-queue counter
+    double2 *d_part;     // [chunk][nsuper][ncomp][K] adjoint partial sums
+
     // workspace
     double2 *d_F;       // [chunk][nchan][nrings][M] ring spectra
     double2 *d_W;       // [chunk][npix] Bluestein accumulation scratch (adjoint, Q > 1)
@@ -114,6 +131,7 @@ int launch_legendre_adjoint(const Plan &p, const double2 *F, double2 *alm, int n
 int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cudaStream_t s);
 int launch_ring_adjoint(const Plan &p, const double *maps, double2 *F, double2 *W, int nb,
                         cudaStream_t s);
+int launch_start_states(const Plan &p, cudaStream_t s);
 int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *offs, int nlen,
                            cudaStream_t s);
 

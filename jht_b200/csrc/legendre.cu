@@ -2,30 +2,48 @@
 //
 // Synthesis (jht _recursion.py:441-469 spin 0, :512-543 spin 2) and its exact
 // transpose (:472-497, :546-572).  For each order m and half-grid ring t the
-// recursion runs over l = lmin..lmax entirely in registers; no lambda table is
-// stored.  One CTA owns the m-pair (m, lmax - m) (equal work: lmax + 2 steps) and
-// sweeps the 2 nside half-grid rings in tiles of NT*R rings, R rings per thread.
+// recursion runs over l entirely in registers; no lambda table is stored.
+//
+// Work decomposition.  A warp tile is 32*R consecutive half-grid rings of one m
+// (R rings per lane, 32 apart).  Persistent warps pull work items from an atomic
+// queue sorted by cost, so the triangle of work over m balances without m-pairing
+// and no CTA-wide barrier ever couples warps:
+//   synthesis: item = (m, warp tile); each item writes its own F[ring][m] entries.
+//   adjoint:   item = (m, quarter of the rings); the warp sweeps its warp tiles in
+//              ascending start-l order and accumulates each l's ring sum into its
+//              own partial row; a final kernel adds the four quarters in fixed
+//              order -- deterministic, no atomics on data.
 //
 // Numerics.  jht carries lambda as (mantissa, log-scale) renormalised every step
-// (_recursion.py:352-369: one sqrt, log, exp and two divisions per step).  Here
-// the recursion is rewritten with per-(l,m) normalised coefficients (plan.cu):
+// (_recursion.py:352-369: one sqrt, log, exp and two divisions per step).  Here the
+// recursion is rewritten with per-(l,m) normalised coefficients (plan.cu):
 //     mu_l = (alpha_l x + gamma_l) mu_{l-1} - mu_{l-2},   lambda_l = c_l mu_l,
-// two FMAs per step, and underflow is handled with an integer scale
-// (value = mu * 2^(800 sc)).  While sc < 0 the value is < 2^-400 and is not
-// accumulated; the rescale check runs only in that phase, which a warp leaves as
-// soon as all its rings reach sc = 0 (then the loop is branch-free).
+// two FMAs per step; underflow is handled with an integer scale (value =
+// mu 2^(800 sc)).  While sc < 0 the value is < 2^-400 and is not accumulated.
+//
+// Dead-work skipping.  For (m, ring) near the poles lambda stays below 2^-400 for
+// the first part of the l range (23% of all (l, m, ring) triples at nside 2048,
+// lmax 4096).  At plan creation start_state_kernel runs that part once per warp
+// tile and stores, at the first l where any ring of the tile is representable
+// (rounded down to an even offset from lmin), every ring's (mu_{l-1}, mu_{l-2}, sc).
+// The transforms then start there; rings still scaled run the rescale-check
+// variant until the whole warp is representable, after which the loop is
+// branch-free.
 //
 // Parity.  Step i = l - lmin alternates between accumulator slots A (i even) and
-// B (i odd); N/S outputs are A +- B, which realises jht's total / signed sums
-// without per-step signs.
+// B (i odd); N/S outputs are A +- B, realising jht's total / signed sums.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "jhtb_internal.cuh"
 
 namespace jhtb {
 namespace {
 
-constexpr int kChunk = 64;  // recursion steps staged in shared memory per round (even)
+constexpr int kWarpsPerBlock = 4;
+constexpr int kStage = 32;  // steps staged per warp per round (one per lane)
+constexpr int kSub = 8;     // adjoint steps per warp reduction
 constexpr unsigned kFull = 0xffffffffu;
 
 struct LegParams {
@@ -34,6 +52,16 @@ struct LegParams {
     const double *x, *logsin, *logch, *logsh;
     const SeedParam *seed;
     const double *alpha, *gamma, *cnorm;
+    // work items
+    int ntiles;               // warp tiles per m
+    int nsuper, tps;          // adjoint: quarters per m, warp tiles per quarter
+    const int *lw;            // [M * ntiles] start l per (m, tile)
+    const double2 *st;        // [M * ntiles][nrec][R][32] start (u1, u2)
+    const int *stsc;          // [M * ntiles][nrec][R][32] start scale
+    const int *synth_order;   // [M * ntiles]
+    const int *adj_order;     // [M * nsuper]
+    const int *adj_tiles;     // [M * nsuper][tps] tile ids, ascending start l, -1 padded
+    unsigned *counter;
 };
 
 LegParams make_params(const Plan &p) {
@@ -52,6 +80,16 @@ LegParams make_params(const Plan &p) {
     q.alpha = p.d_alpha;
     q.gamma = p.d_gamma;
     q.cnorm = p.d_cnorm;
+    q.ntiles = p.ntiles;
+    q.nsuper = p.nsuper;
+    q.tps = p.tps;
+    q.lw = p.d_lw;
+    q.st = p.d_st;
+    q.stsc = p.d_stsc;
+    q.synth_order = p.d_synth_order;
+    q.adj_order = p.d_adj_order;
+    q.adj_tiles = p.d_adj_tiles;
+    q.counter = p.d_counter;
     return q;
 }
 
@@ -83,7 +121,6 @@ __device__ __forceinline__ double seed_log2(const SeedParam &sp, int h, double l
     return v;
 }
 
-// One scaled-phase bookkeeping step: returns the new value and updates prev/sc.
 __device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {
     if (sc < 0 && fabs(u) > kBig) {
         u *= kScaleDown;
@@ -92,9 +129,127 @@ __device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {
     }
 }
 
+__device__ __forceinline__ int next_item(unsigned *counter) {
+    int it = 0;
+    if ((threadIdx.x & 31) == 0) it = (int)atomicAdd(counter, 1u);
+    return __shfl_sync(kFull, it, 0);
+}
+
 // =====================================================================================
-// synthesis, spin 0
+// start states (plan creation): run the scaled recursion of each warp tile up to the
+// first step at which any of its rings is representable.
 // =====================================================================================
+template <int SPIN, int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) start_state_kernel(LegParams p, int nitems) {
+    constexpr int NREC = SPIN ? 2 : 1;
+    const int lane = threadIdx.x & 31;
+    const int item = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    if (item >= nitems) return;
+    const int m = item / p.ntiles, tile = item % p.ntiles;
+    const SeedParam sd = p.seed[m];
+    const long long b0 = alm_index(sd.lmin, m, p.lmax);
+    const int nst = p.lmax - sd.lmin + 1;
+    double x[R], u1[NREC][R], u2[NREC][R];
+    int sc[NREC][R];
+    bool valid[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int t = tile * 32 * R + r * 32 + lane;
+        valid[r] = t < p.T;
+        x[r] = valid[r] ? p.x[t] : 0.0;
+#pragma unroll
+        for (int h = 0; h < NREC; ++h) {
+            double mant = 0.0;
+            int s = 0;
+            if (valid[r]) {
+                const double lg = SPIN ? seed_log2(sd, h, p.logch[t], p.logsh[t]) : seed_log0(sd, m, p.logsin[t]);
+                make_seed(lg, sd.sign[h], mant, s);
+            }
+            u1[h][r] = 0.0;
+            u2[h][r] = -mant;
+            sc[h][r] = s;
+        }
+    }
+    double s1[NREC][R], s2[NREC][R];
+    int ssc[NREC][R];
+    int iw = nst;  // dead unless a ring becomes representable
+    for (int i = 0; i < nst; ++i) {
+        if ((i & 1) == 0) {
+#pragma unroll
+            for (int h = 0; h < NREC; ++h)
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    s1[h][r] = u1[h][r];
+                    s2[h][r] = u2[h][r];
+                    ssc[h][r] = sc[h][r];
+                }
+        }
+        const double al = p.alpha[b0 + i];
+        const double ga = SPIN ? p.gamma[b0 + i] : 0.0;
+        bool sig = false;
+#pragma unroll
+        for (int h = 0; h < NREC; ++h) {
+            const double g = h ? -ga : ga;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                double u = fma(fma(al, x[r], g), u1[h][r], -u2[h][r]);
+                double prev = u1[h][r];
+                rescale(u, prev, sc[h][r]);
+                u2[h][r] = prev;
+                u1[h][r] = u;
+                sig |= valid[r] && sc[h][r] == 0;
+            }
+        }
+        if (__any_sync(kFull, sig)) {
+            iw = i & ~1;
+            break;
+        }
+    }
+    if (lane == 0) const_cast<int *>(p.lw)[item] = sd.lmin + iw;
+    double2 *st = const_cast<double2 *>(p.st) + (size_t)item * NREC * R * 32;
+    int *stsc = const_cast<int *>(p.stsc) + (size_t)item * NREC * R * 32;
+#pragma unroll
+    for (int h = 0; h < NREC; ++h)
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int o = (h * R + r) * 32 + lane;
+            if (iw < nst) {
+                st[o] = make_double2(s1[h][r], s2[h][r]);
+                stsc[o] = valid[r] ? ssc[h][r] : 0;
+            } else {
+                st[o] = make_double2(0.0, 0.0);
+                stsc[o] = 0;
+            }
+        }
+}
+
+// Load the start state of ring slot r for recursion h; invalid rings read (0, 0, 0).
+template <int R>
+__device__ __forceinline__ void load_start(const LegParams &p, int item, int h, int nrec, int lane, double (&u1)[R],
+                                           double (&u2)[R], int (&sc)[R]) {
+    const double2 *st = p.st + (size_t)item * nrec * R * 32;
+    const int *stsc = p.stsc + (size_t)item * nrec * R * 32;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const double2 s = st[(h * R + r) * 32 + lane];
+        u1[r] = s.x;
+        u2[r] = s.y;
+        sc[r] = stsc[(h * R + r) * 32 + lane];
+    }
+}
+
+// =====================================================================================
+// synthesis
+// =====================================================================================
+struct Stage0 {
+    double al[kStage];
+    double2 c[kStage];
+};
+struct Stage2 {
+    double al[kStage], ga[kStage];
+    double2 cp[kStage], cm[kStage];
+};
+
 template <int R, bool SLOW>
 __device__ __forceinline__ void synth0_step(double al, double2 c, const double (&x)[R], double (&u1)[R],
                                             double (&u2)[R], int (&sc)[R], double (&ar)[R], double (&ai)[R]) {
@@ -105,100 +260,88 @@ __device__ __forceinline__ void synth0_step(double al, double2 c, const double (
         if (SLOW) rescale(u, prev, sc[k]);
         u2[k] = prev;
         u1[k] = u;
-        if (!SLOW || sc[k] == 0) {
-            ar[k] = fma(c.x, u, ar[k]);
-            ai[k] = fma(c.y, u, ai[k]);
-        }
+        if (SLOW && sc[k] != 0) u = 0.0;
+        ar[k] = fma(c.x, u, ar[k]);
+        ai[k] = fma(c.y, u, ai[k]);
     }
 }
 
 template <int R, bool SLOW>
-__device__ __forceinline__ void synth0_chunk(int cnt, const double *s_al, const double2 *s_c,
-                                             const double (&x)[R], double (&u1)[R], double (&u2)[R],
-                                             int (&sc)[R], double (&Ar)[R], double (&Ai)[R], double (&Br)[R],
-                                             double (&Bi)[R]) {
+__device__ __forceinline__ void synth0_chunk(int cnt, const Stage0 &sb, const double (&x)[R], double (&u1)[R],
+                                             double (&u2)[R], int (&sc)[R], double (&Ar)[R], double (&Ai)[R],
+                                             double (&Br)[R], double (&Bi)[R]) {
     int q = 0;
     for (; q + 1 < cnt; q += 2) {
-        synth0_step<R, SLOW>(s_al[q], s_c[q], x, u1, u2, sc, Ar, Ai);
-        synth0_step<R, SLOW>(s_al[q + 1], s_c[q + 1], x, u1, u2, sc, Br, Bi);
+        synth0_step<R, SLOW>(sb.al[q], sb.c[q], x, u1, u2, sc, Ar, Ai);
+        synth0_step<R, SLOW>(sb.al[q + 1], sb.c[q + 1], x, u1, u2, sc, Br, Bi);
     }
-    if (q < cnt) synth0_step<R, SLOW>(s_al[q], s_c[q], x, u1, u2, sc, Ar, Ai);
+    if (q < cnt) synth0_step<R, SLOW>(sb.al[q], sb.c[q], x, u1, u2, sc, Ar, Ai);
 }
 
-template <int R, int NT>
-__global__ void __launch_bounds__(NT) synth0_kernel(LegParams p, const double2 *__restrict__ alm_all,
-                                                     double2 *__restrict__ F_all) {
-    __shared__ double s_al[kChunk];
-    __shared__ double2 s_c[kChunk];
-    const int tid = threadIdx.x;
+template <int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) synth0_kernel(LegParams p, const double2 *__restrict__ alm_all,
+                                                                     double2 *__restrict__ F_all, int nb) {
+    __shared__ Stage0 stage[kWarpsPerBlock];
+    const int lane = threadIdx.x & 31;
+    Stage0 &sb = stage[threadIdx.x >> 5];
+    const int nitems = p.M * p.ntiles;
     const int L = p.lmax;
-    const double2 *alm = alm_all + (size_t)blockIdx.y * p.K;
-    double2 *F = F_all + (size_t)blockIdx.y * p.nrings * p.M;
-    const int j = blockIdx.x;
-    for (int pass = 0; pass < 2; ++pass) {
-        const int m = pass ? L - j : j;
-        if (pass && m <= j) break;
-        const SeedParam sp = p.seed[m];
-        const long long b0 = alm_index(sp.lmin, m, L);
-        const int nst = L - sp.lmin + 1;
-        for (int tile = 0; tile < p.T; tile += NT * R) {
-            double x[R], u1[R], u2[R], Ar[R], Ai[R], Br[R], Bi[R];
-            int sc[R];
-            bool fast = true;
+    for (;;) {
+        const int it = next_item(p.counter);
+        if (it >= nitems * nb) break;
+        const int b = it / nitems;
+        const int item = p.synth_order[it - b * nitems];
+        const int m = item / p.ntiles, tile = item % p.ntiles;
+        const double2 *alm = alm_all + (size_t)b * p.K;
+        double2 *F = F_all + (size_t)b * p.nrings * p.M;
+        const SeedParam sd = p.seed[m];
+        const long long b0 = alm_index(sd.lmin, m, L);
+        const int nst = L - sd.lmin + 1;
+        const int i_start = p.lw[item] - sd.lmin;
+        double x[R], u1[R], u2[R], Ar[R], Ai[R], Br[R], Bi[R];
+        int sc[R];
+        load_start<R>(p, item, 0, 1, lane, u1, u2, sc);
+        bool fast = true;
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int t = tile + k * NT + tid;
-                double mant = 0.0, xx = 0.0;
-                int s = 0;
-                if (t < p.T) {
-                    xx = p.x[t];
-                    make_seed(seed_log0(sp, m, p.logsin[t]), sp.sign[0], mant, s);
-                }
-                // (u1, u2) = (0, -seed): the first generic step (alpha = 0) yields the seed.
-                x[k] = xx;
-                u1[k] = 0.0;
-                u2[k] = -mant;
-                sc[k] = s;
-                fast &= (s == 0);
-                Ar[k] = Ai[k] = Br[k] = Bi[k] = 0.0;
+        for (int r = 0; r < R; ++r) {
+            const int t = tile * 32 * R + r * 32 + lane;
+            x[r] = t < p.T ? p.x[t] : 0.0;
+            fast &= sc[r] == 0;
+            Ar[r] = Ai[r] = Br[r] = Bi[r] = 0.0;
+        }
+        for (int i0 = i_start; i0 < nst; i0 += kStage) {
+            const int cnt = min(kStage, nst - i0);
+            if (lane < cnt) {
+                const long long idx = b0 + i0 + lane;
+                const double c = p.cnorm[idx];
+                const double2 a = alm[idx];
+                sb.al[lane] = p.alpha[idx];
+                sb.c[lane] = make_double2(a.x * c, a.y * c);
             }
-            for (int i0 = 0; i0 < nst; i0 += kChunk) {
-                const int cnt = min(kChunk, nst - i0);
-                __syncthreads();
-                for (int q = tid; q < cnt; q += NT) {
-                    const long long idx = b0 + i0 + q;
-                    const double c = p.cnorm[idx];
-                    const double2 a = alm[idx];
-                    s_al[q] = p.alpha[idx];
-                    s_c[q] = make_double2(a.x * c, a.y * c);
-                }
-                __syncthreads();
-                if (__all_sync(kFull, fast)) {
-                    synth0_chunk<R, false>(cnt, s_al, s_c, x, u1, u2, sc, Ar, Ai, Br, Bi);
-                } else {
-                    synth0_chunk<R, true>(cnt, s_al, s_c, x, u1, u2, sc, Ar, Ai, Br, Bi);
-                    fast = true;
+            __syncwarp();
+            if (__all_sync(kFull, fast)) {
+                synth0_chunk<R, false>(cnt, sb, x, u1, u2, sc, Ar, Ai, Br, Bi);
+            } else {
+                synth0_chunk<R, true>(cnt, sb, x, u1, u2, sc, Ar, Ai, Br, Bi);
+                fast = true;
 #pragma unroll
-                    for (int k = 0; k < R; ++k) fast &= (sc[k] == 0);
-                }
+                for (int r = 0; r < R; ++r) fast &= sc[r] == 0;
             }
-            // F_north = A + B; F_south = (-1)^m (E - O) = A - B   (healpix.py:250-253)
+            __syncwarp();
+        }
+        // F_north = A + B; F_south = (-1)^m (E - O) = A - B   (healpix.py:250-253)
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int t = tile + k * NT + tid;
-                if (t < p.T) {
-                    F[(size_t)t * p.M + m] = make_double2(Ar[k] + Br[k], Ai[k] + Bi[k]);
-                    if (t < p.T - 1)
-                        F[(size_t)(4 * p.nside - 2 - t) * p.M + m] = make_double2(Ar[k] - Br[k], Ai[k] - Bi[k]);
-                }
+        for (int r = 0; r < R; ++r) {
+            const int t = tile * 32 * R + r * 32 + lane;
+            if (t < p.T) {
+                F[(size_t)t * p.M + m] = make_double2(Ar[r] + Br[r], Ai[r] + Bi[r]);
+                if (t < p.T - 1)
+                    F[(size_t)(4 * p.nside - 2 - t) * p.M + m] = make_double2(Ar[r] - Br[r], Ai[r] - Bi[r]);
             }
         }
     }
 }
 
-// =====================================================================================
-// synthesis, spin 2: the d^{+2} and d^{-2} recursions advanced together
-// =====================================================================================
 struct Acc2 {
     double ppr, ppi, pmr, pmi, mmr, mmi, mpr, mpi;
 };
@@ -239,99 +382,88 @@ __device__ __forceinline__ void synth2_step(double al, double ga, double2 cp, do
 }
 
 template <int R, bool SLOW>
-__device__ __forceinline__ void synth2_chunk(int cnt, const double *s_al, const double *s_ga, const double2 *s_cp,
-                                             const double2 *s_cm, const double (&x)[R], double (&p1)[R],
+__device__ __forceinline__ void synth2_chunk(int cnt, const Stage2 &sb, const double (&x)[R], double (&p1)[R],
                                              double (&p2)[R], int (&sp)[R], double (&m1)[R], double (&m2)[R],
                                              int (&sm)[R], Acc2 (&acc)[R]) {
     int q = 0;
     for (; q + 1 < cnt; q += 2) {
-        synth2_step<R, SLOW, 1>(s_al[q], s_ga[q], s_cp[q], s_cm[q], x, p1, p2, sp, m1, m2, sm, acc);
-        synth2_step<R, SLOW, -1>(s_al[q + 1], s_ga[q + 1], s_cp[q + 1], s_cm[q + 1], x, p1, p2, sp, m1, m2, sm, acc);
+        synth2_step<R, SLOW, 1>(sb.al[q], sb.ga[q], sb.cp[q], sb.cm[q], x, p1, p2, sp, m1, m2, sm, acc);
+        synth2_step<R, SLOW, -1>(sb.al[q + 1], sb.ga[q + 1], sb.cp[q + 1], sb.cm[q + 1], x, p1, p2, sp, m1, m2, sm, acc);
     }
-    if (q < cnt) synth2_step<R, SLOW, 1>(s_al[q], s_ga[q], s_cp[q], s_cm[q], x, p1, p2, sp, m1, m2, sm, acc);
+    if (q < cnt) synth2_step<R, SLOW, 1>(sb.al[q], sb.ga[q], sb.cp[q], sb.cm[q], x, p1, p2, sp, m1, m2, sm, acc);
 }
 
-template <int R, int NT>
-__global__ void __launch_bounds__(NT) synth2_kernel(LegParams p, const double2 *__restrict__ alm_all,
-                                                     double2 *__restrict__ F_all) {
-    __shared__ double s_al[kChunk], s_ga[kChunk];
-    __shared__ double2 s_cp[kChunk], s_cm[kChunk];
-    const int tid = threadIdx.x;
+template <int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) synth2_kernel(LegParams p, const double2 *__restrict__ alm_all,
+                                                                     double2 *__restrict__ F_all, int nb) {
+    __shared__ Stage2 stage[kWarpsPerBlock];
+    const int lane = threadIdx.x & 31;
+    Stage2 &sb = stage[threadIdx.x >> 5];
+    const int nitems = p.M * p.ntiles;
     const int L = p.lmax;
-    const double2 *aE = alm_all + (size_t)blockIdx.y * 2 * p.K;
-    const double2 *aB = aE + p.K;
-    double2 *Fp = F_all + (size_t)blockIdx.y * 2 * p.nrings * p.M;
-    double2 *Fm = Fp + (size_t)p.nrings * p.M;
-    const int j = blockIdx.x;
-    for (int pass = 0; pass < 2; ++pass) {
-        const int m = pass ? L - j : j;
-        if (pass && m <= j) break;
+    for (;;) {
+        const int it = next_item(p.counter);
+        if (it >= nitems * nb) break;
+        const int b = it / nitems;
+        const int item = p.synth_order[it - b * nitems];
+        const int m = item / p.ntiles, tile = item % p.ntiles;
+        const double2 *aE = alm_all + (size_t)b * 2 * p.K;
+        const double2 *aB = aE + p.K;
+        double2 *Fp = F_all + (size_t)b * 2 * p.nrings * p.M;
+        double2 *Fm = Fp + (size_t)p.nrings * p.M;
         const SeedParam sd = p.seed[m];
         const long long b0 = alm_index(sd.lmin, m, L);
         const int nst = L - sd.lmin + 1;
+        const int i_start = p.lw[item] - sd.lmin;
         // south sign (-1)^(m + lmin): the signed sums are relative to l = lmin
         const double ssign = ((m + sd.lmin) & 1) ? -1.0 : 1.0;
-        for (int tile = 0; tile < p.T; tile += NT * R) {
-            double x[R], p1[R], p2[R], m1[R], m2[R];
-            int sp[R], sm[R];
-            Acc2 acc[R];
-            bool fast = true;
+        double x[R], p1[R], p2[R], m1[R], m2[R];
+        int sp[R], sm[R];
+        Acc2 acc[R];
+        load_start<R>(p, item, 0, 2, lane, p1, p2, sp);
+        load_start<R>(p, item, 1, 2, lane, m1, m2, sm);
+        bool fast = true;
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int t = tile + k * NT + tid;
-                double mp = 0.0, mm = 0.0, xx = 0.0;
-                int s1 = 0, s2 = 0;
-                if (t < p.T) {
-                    xx = p.x[t];
-                    const double lch = p.logch[t], lsh = p.logsh[t];
-                    make_seed(seed_log2(sd, 0, lch, lsh), sd.sign[0], mp, s1);
-                    make_seed(seed_log2(sd, 1, lch, lsh), sd.sign[1], mm, s2);
-                }
-                x[k] = xx;
-                p1[k] = 0.0;
-                p2[k] = -mp;
-                sp[k] = s1;
-                m1[k] = 0.0;
-                m2[k] = -mm;
-                sm[k] = s2;
-                fast &= (s1 == 0) && (s2 == 0);
-                acc[k] = Acc2{0, 0, 0, 0, 0, 0, 0, 0};
+        for (int r = 0; r < R; ++r) {
+            const int t = tile * 32 * R + r * 32 + lane;
+            x[r] = t < p.T ? p.x[t] : 0.0;
+            fast &= (sp[r] == 0) && (sm[r] == 0);
+            acc[r] = Acc2{0, 0, 0, 0, 0, 0, 0, 0};
+        }
+        for (int i0 = i_start; i0 < nst; i0 += kStage) {
+            const int cnt = min(kStage, nst - i0);
+            if (lane < cnt) {
+                const long long idx = b0 + i0 + lane;
+                const double c = p.cnorm[idx];
+                const double2 e = aE[idx], bb = aB[idx];
+                sb.al[lane] = p.alpha[idx];
+                sb.ga[lane] = p.gamma[idx];
+                // cp = -(aE + i aB) c, cm = -(aE - i aB) c   (healpix.py:316-318)
+                sb.cp[lane] = make_double2(-(e.x - bb.y) * c, -(e.y + bb.x) * c);
+                sb.cm[lane] = make_double2(-(e.x + bb.y) * c, -(e.y - bb.x) * c);
             }
-            for (int i0 = 0; i0 < nst; i0 += kChunk) {
-                const int cnt = min(kChunk, nst - i0);
-                __syncthreads();
-                for (int q = tid; q < cnt; q += NT) {
-                    const long long idx = b0 + i0 + q;
-                    const double c = p.cnorm[idx];
-                    const double2 e = aE[idx], b = aB[idx];
-                    s_al[q] = p.alpha[idx];
-                    s_ga[q] = p.gamma[idx];
-                    // cp = -(aE + i aB) c, cm = -(aE - i aB) c   (healpix.py:316-318)
-                    s_cp[q] = make_double2(-(e.x - b.y) * c, -(e.y + b.x) * c);
-                    s_cm[q] = make_double2(-(e.x + b.y) * c, -(e.y - b.x) * c);
-                }
-                __syncthreads();
-                if (__all_sync(kFull, fast)) {
-                    synth2_chunk<R, false>(cnt, s_al, s_ga, s_cp, s_cm, x, p1, p2, sp, m1, m2, sm, acc);
-                } else {
-                    synth2_chunk<R, true>(cnt, s_al, s_ga, s_cp, s_cm, x, p1, p2, sp, m1, m2, sm, acc);
-                    fast = true;
+            __syncwarp();
+            if (__all_sync(kFull, fast)) {
+                synth2_chunk<R, false>(cnt, sb, x, p1, p2, sp, m1, m2, sm, acc);
+            } else {
+                synth2_chunk<R, true>(cnt, sb, x, p1, p2, sp, m1, m2, sm, acc);
+                fast = true;
 #pragma unroll
-                    for (int k = 0; k < R; ++k) fast &= (sp[k] == 0) && (sm[k] == 0);
-                }
+                for (int r = 0; r < R; ++r) fast &= (sp[r] == 0) && (sm[r] == 0);
             }
+            __syncwarp();
+        }
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int t = tile + k * NT + tid;
-                if (t < p.T) {
-                    const Acc2 &a = acc[k];
-                    Fp[(size_t)t * p.M + m] = make_double2(a.ppr, a.ppi);
-                    Fm[(size_t)t * p.M + m] = make_double2(a.mmr, a.mmi);
-                    if (t < p.T - 1) {
-                        const size_t rs = (size_t)(4 * p.nside - 2 - t) * p.M + m;
-                        Fp[rs] = make_double2(ssign * a.pmr, ssign * a.pmi);
-                        Fm[rs] = make_double2(ssign * a.mpr, ssign * a.mpi);
-                    }
+        for (int r = 0; r < R; ++r) {
+            const int t = tile * 32 * R + r * 32 + lane;
+            if (t < p.T) {
+                const Acc2 &a = acc[r];
+                Fp[(size_t)t * p.M + m] = make_double2(a.ppr, a.ppi);
+                Fm[(size_t)t * p.M + m] = make_double2(a.mmr, a.mmi);
+                if (t < p.T - 1) {
+                    const size_t rs = (size_t)(4 * p.nside - 2 - t) * p.M + m;
+                    Fp[rs] = make_double2(ssign * a.pmr, ssign * a.pmi);
+                    Fm[rs] = make_double2(ssign * a.mpr, ssign * a.mpi);
                 }
             }
         }
@@ -339,14 +471,9 @@ __global__ void __launch_bounds__(NT) synth2_kernel(LegParams p, const double2 *
 }
 
 // =====================================================================================
-// adjoint: per-step partial sums over the thread's rings, reduced across the warp
-// (butterfly reduce-scatter), across warps (shared memory, fixed order) and across
-// ring tiles (accumulated in the output by the owning CTA) -- deterministic.
+// adjoint
 // =====================================================================================
-constexpr int kSub = 8;  // steps per warp reduction
-
-// After the call, lane l holds in v[0] the warp total of entry idx(l) where, for
-// NV = 8: idx = ((l>>4)&1)*4 + ((l>>3)&1)*2 + ((l>>2)&1); for NV = 16 one more bit.
+// After the call, lane l holds in v[0] the warp total of entry scatter_index(l).
 template <int NV>
 __device__ __forceinline__ void warp_reduce_scatter(double2 (&v)[NV], int lane) {
     int mask = 16;
@@ -378,16 +505,19 @@ __device__ __forceinline__ int scatter_index(int lane) {
 
 template <int NV>
 __device__ __forceinline__ bool scatter_writer(int lane) {
-    // lanes whose bits below the scatter bits are zero
     constexpr int used = NV == 8 ? 3 : (NV == 16 ? 4 : 5);
     return (lane & ((1 << (5 - used)) - 1)) == 0;
 }
+
+struct AStage {
+    double al[kStage], ga[kStage];
+};
 
 // ---------------- spin 0 ----------------
 template <int R, bool SLOW>
 __device__ __forceinline__ double2 adj0_step(double al, const double (&x)[R], double (&u1)[R], double (&u2)[R],
                                              int (&sc)[R], const double2 (&U)[R]) {
-    double2 part = make_double2(0.0, 0.0);
+    double2 part[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         double u = fma(al * x[k], u1[k], -u2[k]);
@@ -396,110 +526,109 @@ __device__ __forceinline__ double2 adj0_step(double al, const double (&x)[R], do
         u2[k] = prev;
         u1[k] = u;
         if (SLOW && sc[k] != 0) u = 0.0;
-        part.x = fma(u, U[k].x, part.x);
-        part.y = fma(u, U[k].y, part.y);
+        part[k] = make_double2(u * U[k].x, u * U[k].y);
     }
-    return part;
-}
-
-template <int R, bool SLOW>
-__device__ __forceinline__ void adj0_sub(int cnt, const double *s_al, const double (&x)[R], double (&u1)[R],
-                                         double (&u2)[R], int (&sc)[R], const double2 (&UA)[R],
-                                         const double2 (&UB)[R], double2 (&part)[kSub]) {
 #pragma unroll
-    for (int q = 0; q < kSub; q += 2) {
-        if (q < cnt) part[q] = adj0_step<R, SLOW>(s_al[q], x, u1, u2, sc, UA);
-        else part[q] = make_double2(0.0, 0.0);
-        if (q + 1 < cnt) part[q + 1] = adj0_step<R, SLOW>(s_al[q + 1], x, u1, u2, sc, UB);
-        else part[q + 1] = make_double2(0.0, 0.0);
-    }
+    for (int s = 1; s < R; s *= 2)
+#pragma unroll
+        for (int k = 0; k + s < R; k += 2 * s) {
+            part[k].x += part[k + s].x;
+            part[k].y += part[k + s].y;
+        }
+    return part[0];
 }
 
-template <int R, int NT>
-__global__ void __launch_bounds__(NT) adj0_kernel(LegParams p, const double2 *__restrict__ V_all,
-                                                   double2 *__restrict__ alm_all) {
-    constexpr int NW = NT / 32;
-    __shared__ double s_al[kChunk], s_c[kChunk];
-    __shared__ double2 s_red[NW][kChunk];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+template <int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) adj0_kernel(LegParams p, const double2 *__restrict__ V_all,
+                                                                   double2 *__restrict__ part_all, int nb) {
+    __shared__ AStage stage[kWarpsPerBlock];
+    const int lane = threadIdx.x & 31;
+    AStage &sb = stage[threadIdx.x >> 5];
+    const int nsup = p.M * p.nsuper;
     const int L = p.lmax;
-    const double2 *V = V_all + (size_t)blockIdx.y * p.nrings * p.M;
-    double2 *alm = alm_all + (size_t)blockIdx.y * p.K;
-    const int j = blockIdx.x;
-    for (int pass = 0; pass < 2; ++pass) {
-        const int m = pass ? L - j : j;
-        if (pass && m <= j) break;
-        const SeedParam sp = p.seed[m];
-        const long long b0 = alm_index(sp.lmin, m, L);
-        const int nst = L - sp.lmin + 1;
-        for (int tile = 0; tile < p.T; tile += NT * R) {
+    for (;;) {
+        const int it = next_item(p.counter);
+        if (it >= nsup * nb) break;
+        const int b = it / nsup;
+        const int sitem = p.adj_order[it - b * nsup];
+        const int m = sitem / p.nsuper, s = sitem % p.nsuper;
+        const double2 *V = V_all + (size_t)b * p.nrings * p.M;
+        double2 *part = part_all + ((size_t)b * p.nsuper + s) * p.K;
+        const SeedParam sd = p.seed[m];
+        const long long b0 = alm_index(sd.lmin, m, L);
+        const int nst = L - sd.lmin + 1;
+        bool any = false;  // a live tile has already written the row
+        for (int j = 0; j < p.tps; ++j) {
+            const int tile = p.adj_tiles[(size_t)sitem * p.tps + j];
+            if (tile < 0) break;
+            const int item = m * p.ntiles + tile;
+            const int i_start = p.lw[item] - sd.lmin;
+            if (i_start >= nst) break;  // ascending order: the rest are dead too
+            const bool acc = any;       // later tiles add onto the row (their range is inside)
+            if (!any)                   // first live tile: zero the prefix no tile reaches
+                for (int i = lane; i < i_start; i += 32) part[b0 + i] = make_double2(0.0, 0.0);
             double x[R], u1[R], u2[R];
             int sc[R];
             double2 UA[R], UB[R];
+            load_start<R>(p, item, 0, 1, lane, u1, u2, sc);
             bool fast = true;
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int t = tile + k * NT + tid;
-                double mant = 0.0, xx = 0.0;
-                int s = 0;
+            for (int r = 0; r < R; ++r) {
+                const int t = tile * 32 * R + r * 32 + lane;
                 double2 vn = make_double2(0.0, 0.0), vs = make_double2(0.0, 0.0);
+                x[r] = 0.0;
                 if (t < p.T) {
-                    xx = p.x[t];
-                    make_seed(seed_log0(sp, m, p.logsin[t]), sp.sign[0], mant, s);
+                    x[r] = p.x[t];
                     vn = V[(size_t)t * p.M + m];
                     if (t < p.T - 1) vs = V[(size_t)(4 * p.nside - 2 - t) * p.M + m];
                 }
-                // b_l = sum_t lambda (Vn + (-1)^l (-1)^m V_south)  (_recursion.py:472-497, healpix.py:255-258)
-                x[k] = xx;
-                u1[k] = 0.0;
-                u2[k] = -mant;
-                sc[k] = s;
-                fast &= (s == 0);
-                UA[k] = make_double2(vn.x + vs.x, vn.y + vs.y);
-                UB[k] = make_double2(vn.x - vs.x, vn.y - vs.y);
+                // b_l = sum_t lambda (Vn + (-1)^l (-1)^m V_south)  (_recursion.py:472-497)
+                UA[r] = make_double2(vn.x + vs.x, vn.y + vs.y);
+                UB[r] = make_double2(vn.x - vs.x, vn.y - vs.y);
+                fast &= sc[r] == 0;
             }
-            for (int i0 = 0; i0 < nst; i0 += kChunk) {
-                const int cnt = min(kChunk, nst - i0);
-                __syncthreads();
-                for (int q = tid; q < cnt; q += NT) {
-                    const long long idx = b0 + i0 + q;
-                    s_al[q] = p.alpha[idx];
-                    s_c[q] = p.cnorm[idx];
-                }
-                __syncthreads();
+            for (int i0 = i_start; i0 < nst; i0 += kStage) {
+                const int cnt = min(kStage, nst - i0);
+                if (lane < cnt) sb.al[lane] = p.alpha[b0 + i0 + lane];
+                __syncwarp();
                 for (int q0 = 0; q0 < cnt; q0 += kSub) {
-                    double2 part[kSub];
-                    if (__all_sync(kFull, fast)) {
-                        adj0_sub<R, false>(cnt - q0, s_al + q0, x, u1, u2, sc, UA, UB, part);
-                    } else {
-                        adj0_sub<R, true>(cnt - q0, s_al + q0, x, u1, u2, sc, UA, UB, part);
+                    double2 v[kSub];
+                    const bool f = __all_sync(kFull, fast);
+#pragma unroll
+                    for (int q = 0; q < kSub; q += 2) {
+                        if (q0 + q < cnt)
+                            v[q] = f ? adj0_step<R, false>(sb.al[q0 + q], x, u1, u2, sc, UA)
+                                     : adj0_step<R, true>(sb.al[q0 + q], x, u1, u2, sc, UA);
+                        else v[q] = make_double2(0.0, 0.0);
+                        if (q0 + q + 1 < cnt)
+                            v[q + 1] = f ? adj0_step<R, false>(sb.al[q0 + q + 1], x, u1, u2, sc, UB)
+                                         : adj0_step<R, true>(sb.al[q0 + q + 1], x, u1, u2, sc, UB);
+                        else v[q + 1] = make_double2(0.0, 0.0);
+                    }
+                    if (!f) {
                         fast = true;
 #pragma unroll
-                        for (int k = 0; k < R; ++k) fast &= (sc[k] == 0);
+                        for (int r = 0; r < R; ++r) fast &= sc[r] == 0;
                     }
-                    warp_reduce_scatter<kSub>(part, lane);
-                    if (scatter_writer<kSub>(lane)) s_red[warp][q0 + scatter_index<kSub>(lane)] = part[0];
+                    warp_reduce_scatter<kSub>(v, lane);
+                    const int q = q0 + scatter_index<kSub>(lane);
+                    if (scatter_writer<kSub>(lane) && q < cnt) {
+                        const long long idx = b0 + i0 + q;
+                        double2 o = v[0];
+                        if (acc) {
+                            const double2 prev = part[idx];
+                            o.x += prev.x;
+                            o.y += prev.y;
+                        }
+                        part[idx] = o;
+                    }
                 }
-                __syncthreads();
-                for (int q = tid; q < cnt; q += NT) {
-                    double2 s = s_red[0][q];
-#pragma unroll
-                    for (int w = 1; w < NW; ++w) {
-                        s.x += s_red[w][q].x;
-                        s.y += s_red[w][q].y;
-                    }
-                    const double c = s_c[q];
-                    const long long idx = b0 + i0 + q;
-                    double2 o = make_double2(c * s.x, c * s.y);
-                    if (tile > 0) {
-                        const double2 prev = alm[idx];
-                        o.x += prev.x;
-                        o.y += prev.y;
-                    }
-                    alm[idx] = o;
-                }
+                __syncwarp();
             }
+            any = true;
         }
+        if (!any)  // no live tile: the whole row is zero
+            for (int i = lane; i < nst; i += 32) part[b0 + i] = make_double2(0.0, 0.0);
     }
 }
 
@@ -512,22 +641,21 @@ template <int R, bool SLOW, int SGN>
 __device__ __forceinline__ void adj2_step(double al, double ga, const double (&x)[R], double (&p1)[R],
                                           double (&p2)[R], int (&sp)[R], double (&m1)[R], double (&m2)[R],
                                           int (&sm)[R], const In2 (&in)[R], double2 &op, double2 &om) {
-    op = make_double2(0.0, 0.0);
-    om = make_double2(0.0, 0.0);
+    double2 pp[R], pm[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const double tp = fma(al, x[k], ga);
         const double tm = fma(al, x[k], -ga);
         double up = fma(tp, p1[k], -p2[k]);
         double um = fma(tm, m1[k], -m2[k]);
-        double pp = p1[k], pm = m1[k];
+        double qp = p1[k], qm = m1[k];
         if (SLOW) {
-            rescale(up, pp, sp[k]);
-            rescale(um, pm, sm[k]);
+            rescale(up, qp, sp[k]);
+            rescale(um, qm, sm[k]);
         }
-        p2[k] = pp;
+        p2[k] = qp;
         p1[k] = up;
-        m2[k] = pm;
+        m2[k] = qm;
         m1[k] = um;
         if (SLOW) {
             if (sp[k] != 0) up = 0.0;
@@ -535,174 +663,246 @@ __device__ __forceinline__ void adj2_step(double al, double ga, const double (&x
         }
         const In2 &d = in[k];
         // p2 += lp Vpn + (-1)^l lm Sp ;  m2 += lm Vmn + (-1)^l lp Sm   (_recursion.py:565-566)
-        op.x = fma(up, d.vpn.x, op.x);
-        op.y = fma(up, d.vpn.y, op.y);
-        op.x = fma(SGN * um, d.spA.x, op.x);
-        op.y = fma(SGN * um, d.spA.y, op.y);
-        om.x = fma(um, d.vmn.x, om.x);
-        om.y = fma(um, d.vmn.y, om.y);
-        om.x = fma(SGN * up, d.smA.x, om.x);
-        om.y = fma(SGN * up, d.smA.y, om.y);
+        pp[k] = make_double2(fma(up, d.vpn.x, SGN * um * d.spA.x), fma(up, d.vpn.y, SGN * um * d.spA.y));
+        pm[k] = make_double2(fma(um, d.vmn.x, SGN * up * d.smA.x), fma(um, d.vmn.y, SGN * up * d.smA.y));
     }
-}
-
-template <int R, bool SLOW>
-__device__ __forceinline__ void adj2_sub(int cnt, const double *s_al, const double *s_ga, const double (&x)[R],
-                                         double (&p1)[R], double (&p2)[R], int (&sp)[R], double (&m1)[R],
-                                         double (&m2)[R], int (&sm)[R], const In2 (&in)[R],
-                                         double2 (&part)[2 * kSub]) {
 #pragma unroll
-    for (int q = 0; q < kSub; q += 2) {
-        if (q < cnt) adj2_step<R, SLOW, 1>(s_al[q], s_ga[q], x, p1, p2, sp, m1, m2, sm, in, part[q], part[kSub + q]);
-        else part[q] = part[kSub + q] = make_double2(0.0, 0.0);
-        if (q + 1 < cnt)
-            adj2_step<R, SLOW, -1>(s_al[q + 1], s_ga[q + 1], x, p1, p2, sp, m1, m2, sm, in, part[q + 1],
-                                   part[kSub + q + 1]);
-        else part[q + 1] = part[kSub + q + 1] = make_double2(0.0, 0.0);
-    }
+    for (int s = 1; s < R; s *= 2)
+#pragma unroll
+        for (int k = 0; k + s < R; k += 2 * s) {
+            pp[k].x += pp[k + s].x;
+            pp[k].y += pp[k + s].y;
+            pm[k].x += pm[k + s].x;
+            pm[k].y += pm[k + s].y;
+        }
+    op = pp[0];
+    om = pm[0];
 }
 
-template <int R, int NT>
-__global__ void __launch_bounds__(NT) adj2_kernel(LegParams p, const double2 *__restrict__ V_all,
-                                                   double2 *__restrict__ alm_all) {
-    constexpr int NW = NT / 32;
-    __shared__ double s_al[kChunk], s_ga[kChunk], s_c[kChunk];
-    __shared__ double2 s_red[NW][2 * kChunk];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+template <int R>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) adj2_kernel(LegParams p, const double2 *__restrict__ V_all,
+                                                                   double2 *__restrict__ part_all, int nb) {
+    constexpr int NV = 2 * kSub;
+    __shared__ AStage stage[kWarpsPerBlock];
+    const int lane = threadIdx.x & 31;
+    AStage &sb = stage[threadIdx.x >> 5];
+    const int nsup = p.M * p.nsuper;
     const int L = p.lmax;
-    const double2 *Vp = V_all + (size_t)blockIdx.y * 2 * p.nrings * p.M;
-    const double2 *Vm = Vp + (size_t)p.nrings * p.M;
-    double2 *aE = alm_all + (size_t)blockIdx.y * 2 * p.K;
-    double2 *aB = aE + p.K;
-    const int j = blockIdx.x;
-    for (int pass = 0; pass < 2; ++pass) {
-        const int m = pass ? L - j : j;
-        if (pass && m <= j) break;
+    for (;;) {
+        const int it = next_item(p.counter);
+        if (it >= nsup * nb) break;
+        const int b = it / nsup;
+        const int sitem = p.adj_order[it - b * nsup];
+        const int m = sitem / p.nsuper, s = sitem % p.nsuper;
+        const double2 *Vp = V_all + (size_t)b * 2 * p.nrings * p.M;
+        const double2 *Vm = Vp + (size_t)p.nrings * p.M;
+        double2 *partP = part_all + ((size_t)b * p.nsuper + s) * 2 * p.K;
+        double2 *partM = partP + p.K;
         const SeedParam sd = p.seed[m];
         const long long b0 = alm_index(sd.lmin, m, L);
         const int nst = L - sd.lmin + 1;
         const double ssign = ((m + sd.lmin) & 1) ? -1.0 : 1.0;
-        // modes l in [m, lmin) do not exist for spin 2: zero them
-        if (tid < sd.lmin - m) {
-            const long long idx = alm_index(m + tid, m, L);
-            aE[idx] = make_double2(0.0, 0.0);
-            aB[idx] = make_double2(0.0, 0.0);
-        }
-        for (int tile = 0; tile < p.T; tile += NT * R) {
+        bool any = false;
+        for (int j = 0; j < p.tps; ++j) {
+            const int tile = p.adj_tiles[(size_t)sitem * p.tps + j];
+            if (tile < 0) break;
+            const int item = m * p.ntiles + tile;
+            const int i_start = p.lw[item] - sd.lmin;
+            if (i_start >= nst) break;
+            const bool acc = any;
+            if (!any)
+                for (int i = lane; i < i_start; i += 32) {
+                    partP[b0 + i] = make_double2(0.0, 0.0);
+                    partM[b0 + i] = make_double2(0.0, 0.0);
+                }
             double x[R], p1[R], p2[R], m1[R], m2[R];
             int sp[R], sm[R];
             In2 in[R];
+            load_start<R>(p, item, 0, 2, lane, p1, p2, sp);
+            load_start<R>(p, item, 1, 2, lane, m1, m2, sm);
             bool fast = true;
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const int t = tile + k * NT + tid;
-                double mp = 0.0, mm = 0.0, xx = 0.0;
-                int s1 = 0, s2 = 0;
+            for (int r = 0; r < R; ++r) {
+                const int t = tile * 32 * R + r * 32 + lane;
                 In2 d;
                 d.vpn = d.spA = d.vmn = d.smA = make_double2(0.0, 0.0);
+                x[r] = 0.0;
                 if (t < p.T) {
-                    xx = p.x[t];
-                    const double lch = p.logch[t], lsh = p.logsh[t];
-                    make_seed(seed_log2(sd, 0, lch, lsh), sd.sign[0], mp, s1);
-                    make_seed(seed_log2(sd, 1, lch, lsh), sd.sign[1], mm, s2);
+                    x[r] = p.x[t];
                     d.vpn = Vp[(size_t)t * p.M + m];
                     d.vmn = Vm[(size_t)t * p.M + m];
                     if (t < p.T - 1) {
                         const size_t rs = (size_t)(4 * p.nside - 2 - t) * p.M + m;
-                        const double2 a = Vp[rs], b = Vm[rs];
+                        const double2 a = Vp[rs], c = Vm[rs];
                         d.spA = make_double2(ssign * a.x, ssign * a.y);
-                        d.smA = make_double2(ssign * b.x, ssign * b.y);
+                        d.smA = make_double2(ssign * c.x, ssign * c.y);
                     }
                 }
-                x[k] = xx;
-                p1[k] = 0.0;
-                p2[k] = -mp;
-                sp[k] = s1;
-                m1[k] = 0.0;
-                m2[k] = -mm;
-                sm[k] = s2;
-                fast &= (s1 == 0) && (s2 == 0);
-                in[k] = d;
+                in[r] = d;
+                fast &= (sp[r] == 0) && (sm[r] == 0);
             }
-            for (int i0 = 0; i0 < nst; i0 += kChunk) {
-                const int cnt = min(kChunk, nst - i0);
-                __syncthreads();
-                for (int q = tid; q < cnt; q += NT) {
-                    const long long idx = b0 + i0 + q;
-                    s_al[q] = p.alpha[idx];
-                    s_ga[q] = p.gamma[idx];
-                    s_c[q] = p.cnorm[idx];
+            for (int i0 = i_start; i0 < nst; i0 += kStage) {
+                const int cnt = min(kStage, nst - i0);
+                if (lane < cnt) {
+                    sb.al[lane] = p.alpha[b0 + i0 + lane];
+                    sb.ga[lane] = p.gamma[b0 + i0 + lane];
                 }
-                __syncthreads();
+                __syncwarp();
                 for (int q0 = 0; q0 < cnt; q0 += kSub) {
-                    double2 part[2 * kSub];
-                    if (__all_sync(kFull, fast)) {
-                        adj2_sub<R, false>(cnt - q0, s_al + q0, s_ga + q0, x, p1, p2, sp, m1, m2, sm, in, part);
-                    } else {
-                        adj2_sub<R, true>(cnt - q0, s_al + q0, s_ga + q0, x, p1, p2, sp, m1, m2, sm, in, part);
+                    double2 v[NV];
+                    const bool f = __all_sync(kFull, fast);
+#pragma unroll
+                    for (int q = 0; q < kSub; q += 2) {
+                        if (q0 + q < cnt) {
+                            if (f) adj2_step<R, false, 1>(sb.al[q0 + q], sb.ga[q0 + q], x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
+                            else adj2_step<R, true, 1>(sb.al[q0 + q], sb.ga[q0 + q], x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
+                        } else {
+                            v[q] = v[kSub + q] = make_double2(0.0, 0.0);
+                        }
+                        if (q0 + q + 1 < cnt) {
+                            if (f) adj2_step<R, false, -1>(sb.al[q0 + q + 1], sb.ga[q0 + q + 1], x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
+                            else adj2_step<R, true, -1>(sb.al[q0 + q + 1], sb.ga[q0 + q + 1], x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
+                        } else {
+                            v[q + 1] = v[kSub + q + 1] = make_double2(0.0, 0.0);
+                        }
+                    }
+                    if (!f) {
                         fast = true;
 #pragma unroll
-                        for (int k = 0; k < R; ++k) fast &= (sp[k] == 0) && (sm[k] == 0);
+                        for (int r = 0; r < R; ++r) fast &= (sp[r] == 0) && (sm[r] == 0);
                     }
-                    warp_reduce_scatter<2 * kSub>(part, lane);
-                    if (scatter_writer<2 * kSub>(lane)) {
-                        const int e = scatter_index<2 * kSub>(lane);  // 0..7: p2, 8..15: m2
-                        s_red[warp][(e >= kSub ? kChunk : 0) + q0 + (e & (kSub - 1))] = part[0];
+                    warp_reduce_scatter<NV>(v, lane);
+                    if (scatter_writer<NV>(lane)) {
+                        const int e = scatter_index<NV>(lane);  // 0..7: p2, 8..15: m2
+                        const int q = q0 + (e & (kSub - 1));
+                        if (q < cnt) {
+                            double2 *dst = e >= kSub ? partM : partP;
+                            const long long idx = b0 + i0 + q;
+                            double2 o = v[0];
+                            if (acc) {
+                                const double2 prev = dst[idx];
+                                o.x += prev.x;
+                                o.y += prev.y;
+                            }
+                            dst[idx] = o;
+                        }
                     }
                 }
-                __syncthreads();
-                for (int q = tid; q < cnt; q += NT) {
-                    double2 sp2 = s_red[0][q], sm2 = s_red[0][kChunk + q];
-#pragma unroll
-                    for (int w = 1; w < NW; ++w) {
-                        sp2.x += s_red[w][q].x;
-                        sp2.y += s_red[w][q].y;
-                        sm2.x += s_red[w][kChunk + q].x;
-                        sm2.y += s_red[w][kChunk + q].y;
-                    }
-                    const double c = s_c[q];
-                    const long long idx = b0 + i0 + q;
-                    // aE = (-p2 - m2)/2, aB = i (p2 - m2)/2  (healpix.py:353-354)
-                    const double pr = c * sp2.x, pi = c * sp2.y, mr = c * sm2.x, mi = c * sm2.y;
-                    double2 e = make_double2(0.5 * (-pr - mr), 0.5 * (-pi - mi));
-                    double2 b = make_double2(0.5 * (-(pi - mi)), 0.5 * (pr - mr));
-                    if (tile > 0) {
-                        const double2 pe = aE[idx], pb = aB[idx];
-                        e.x += pe.x;
-                        e.y += pe.y;
-                        b.x += pb.x;
-                        b.y += pb.y;
-                    }
-                    aE[idx] = e;
-                    aB[idx] = b;
-                }
+                __syncwarp();
             }
+            any = true;
+        }
+        if (!any)
+            for (int i = lane; i < nst; i += 32) {
+                partP[b0 + i] = make_double2(0.0, 0.0);
+                partM[b0 + i] = make_double2(0.0, 0.0);
+            }
+    }
+}
+
+// Final adjoint combine: sum the ring quarters in fixed order, scale by c_l and,
+// for spin 2, form aE = (-p2 - m2)/2, aB = i (p2 - m2)/2 (healpix.py:353-354).
+template <int SPIN>
+__global__ void adj_reduce_kernel(int lmax, long long K, int nsuper, const SeedParam *__restrict__ seed,
+                                  const double *__restrict__ cnorm, const double2 *__restrict__ part_all,
+                                  double2 *__restrict__ alm_all, int nb) {
+    constexpr int NC = SPIN ? 2 : 1;
+    const long long total = (long long)nb * K;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(g / K);
+        const long long idx = g - (long long)b * K;
+        // (l, m) of the packed index: m from the column base
+        int m = (int)floor(((2.0 * lmax + 3.0) - sqrt((2.0 * lmax + 3.0) * (2.0 * lmax + 3.0) - 8.0 * (double)idx)) / 2.0);
+        if (m < 0) m = 0;
+        while (m > 0 && alm_index(m, m, lmax) > idx) --m;
+        while (m < lmax && alm_index(m + 1, m + 1, lmax) <= idx) ++m;
+        const int l = (int)(idx - alm_index(0, m, lmax));
+        double2 *out = alm_all + (size_t)b * NC * K;
+        if (l < seed[m].lmin) {
+            out[idx] = make_double2(0.0, 0.0);
+            if (SPIN) out[K + idx] = make_double2(0.0, 0.0);
+            continue;
+        }
+        const double2 *part = part_all + (size_t)b * nsuper * NC * K;
+        double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
+        for (int s = 0; s < nsuper; ++s) {
+            const double2 a = part[(size_t)s * NC * K + idx];
+            s0.x += a.x;
+            s0.y += a.y;
+            if (SPIN) {
+                const double2 c = part[(size_t)s * NC * K + K + idx];
+                s1.x += c.x;
+                s1.y += c.y;
+            }
+        }
+        const double c = cnorm[idx];
+        if (!SPIN) {
+            out[idx] = make_double2(c * s0.x, c * s0.y);
+        } else {
+            const double pr = c * s0.x, pi = c * s0.y, mr = c * s1.x, mi = c * s1.y;
+            out[idx] = make_double2(0.5 * (-pr - mr), 0.5 * (-pi - mi));
+            out[K + idx] = make_double2(0.5 * (-(pi - mi)), 0.5 * (pr - mr));
         }
     }
 }
 
-constexpr int kNT = 256;
-constexpr int kR0 = 4;  // rings per thread, spin 0
-constexpr int kR2 = 2;  // rings per thread, spin 2
+int persistent_grid(int blocks_per_sm) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm * blocks_per_sm;
+}
+
+template <typename Kern>
+int resident_blocks(Kern k) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kWarpsPerBlock * 32, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
 
 }  // namespace
 
+int launch_start_states(const Plan &p, cudaStream_t s) {
+    const int nitems = p.M * p.ntiles;
+    const int grid = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    LegParams q = make_params(p);
+    if (p.spin == 0) start_state_kernel<0, kR0><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
+    else start_state_kernel<2, kR2><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
+    JHTB_CUDA_TRY(cudaGetLastError());
+    return JHTB_OK;
+}
+
 int launch_legendre_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;
-    dim3 grid(p.npairs, nb);
+    JHTB_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned), s));
     LegParams q = make_params(p);
-    if (p.spin == 0) synth0_kernel<kR0, kNT><<<grid, kNT, 0, s>>>(q, alm, F);
-    else synth2_kernel<kR2, kNT><<<grid, kNT, 0, s>>>(q, alm, F);
+    if (p.spin == 0) {
+        auto k = synth0_kernel<kR0>;
+        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, alm, F, nb);
+    } else {
+        auto k = synth2_kernel<kR2>;
+        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, alm, F, nb);
+    }
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
 }
 
 int launch_legendre_adjoint(const Plan &p, const double2 *F, double2 *alm, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;
-    dim3 grid(p.npairs, nb);
+    JHTB_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned), s));
     LegParams q = make_params(p);
-    if (p.spin == 0) adj0_kernel<kR0, kNT><<<grid, kNT, 0, s>>>(q, F, alm);
-    else adj2_kernel<kR2, kNT><<<grid, kNT, 0, s>>>(q, F, alm);
+    if (p.spin == 0) {
+        auto k = adj0_kernel<kR0>;
+        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
+    } else {
+        auto k = adj2_kernel<kR2>;
+        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
+    }
+    JHTB_CUDA_TRY(cudaGetLastError());
+    const long long total = (long long)nb * p.K;
+    const int grid = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
+    if (p.spin == 0) adj_reduce_kernel<0><<<grid, 256, 0, s>>>(p.lmax, p.K, p.nsuper, p.d_seed, p.d_cnorm, p.d_part, alm, nb);
+    else adj_reduce_kernel<2><<<grid, 256, 0, s>>>(p.lmax, p.K, p.nsuper, p.d_seed, p.d_cnorm, p.d_part, alm, nb);
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
 }

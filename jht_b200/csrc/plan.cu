@@ -85,7 +85,8 @@ void free_plan(Plan *p) {
     if (!p) return;
     void *ptrs[] = {p->d_x,     p->d_logsin, p->d_logch, p->d_logsh,   p->d_rings, p->d_tw,
                     p->d_bh,    p->d_seed,   p->d_alpha, p->d_gamma,   p->d_cnorm, p->d_F,
-                    p->d_W,     p->d_scratch};
+                    p->d_W,     p->d_scratch, p->d_lw, p->d_st, p->d_stsc, p->d_synth_order,
+                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : p->events) {
@@ -206,6 +207,52 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     if (spin && (rc = upload(&p->d_gamma, gamma, bytes))) return rc;
     if ((rc = upload(&p->d_cnorm, cnorm, bytes))) return rc;
 
+    // ---- Legendre work items: start states at the first representable l per warp tile,
+    //      cost-sorted orders for the persistent synthesis / adjoint kernels ----------------
+    {
+        const int R = spin ? kR2 : kR0;
+        const int nrec = spin ? 2 : 1;
+        p->ntiles = (T + 32 * R - 1) / (32 * R);
+        p->nsuper = std::min(4, p->ntiles);
+        p->tps = (p->ntiles + p->nsuper - 1) / p->nsuper;
+        const long long nitems = (long long)M * p->ntiles;
+        const size_t nst_el = (size_t)nitems * nrec * R * 32;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_lw, sizeof(int) * nitems));
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_st, sizeof(double2) * nst_el));
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_stsc, sizeof(int) * nst_el));
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_counter, 4 * sizeof(unsigned)));
+        bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nst_el + 4 * sizeof(unsigned);
+        if ((rc = launch_start_states(*p, 0))) return rc;
+        JHTB_CUDA_TRY(cudaDeviceSynchronize());
+        std::vector<int> lw(nitems);
+        JHTB_CUDA_TRY(cudaMemcpy(lw.data(), p->d_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
+        auto cost = [&](long long it) { return std::max(0, L + 1 - lw[it]); };
+        std::vector<int> so(nitems);
+        for (long long i = 0; i < nitems; ++i) so[i] = (int)i;
+        std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return cost(a) > cost(b); });
+        const long long nsup = (long long)M * p->nsuper;
+        std::vector<int> at((size_t)nsup * p->tps, -1), ao(nsup);
+        std::vector<long long> acost(nsup, 0);
+        for (int m = 0; m < M; ++m)
+            for (int s = 0; s < p->nsuper; ++s) {
+                std::vector<int> tl;
+                for (int t = s * p->tps; t < std::min((s + 1) * p->tps, p->ntiles); ++t) tl.push_back(t);
+                std::stable_sort(tl.begin(), tl.end(), [&](int a, int b) {
+                    return lw[(long long)m * p->ntiles + a] < lw[(long long)m * p->ntiles + b];
+                });
+                const long long si = (long long)m * p->nsuper + s;
+                for (size_t j = 0; j < tl.size(); ++j) {
+                    at[si * p->tps + j] = tl[j];
+                    acost[si] += cost((long long)m * p->ntiles + tl[j]);
+                }
+                ao[si] = (int)si;
+            }
+        std::stable_sort(ao.begin(), ao.end(), [&](int a, int b) { return acost[a] > acost[b]; });
+        if ((rc = upload(&p->d_synth_order, so, bytes))) return rc;
+        if ((rc = upload(&p->d_adj_order, ao, bytes))) return rc;
+        if ((rc = upload(&p->d_adj_tiles, at, bytes))) return rc;
+    }
+
     // ---- ring FFT descriptors -------------------------------------------------------------
     std::vector<RingDesc> rings(nr);
     std::map<long long, long long> bh_offset;  // Bluestein length -> offset
@@ -257,6 +304,11 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     p->chunk = std::max(1, p->max_batch);
     JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_F, f_per_map * p->chunk));
     bytes += f_per_map * p->chunk;
+    {
+        const size_t part = sizeof(double2) * (size_t)p->nsuper * p->ncomp * p->K * p->chunk;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_part, part));
+        bytes += part;
+    }
     bool need_w = false;
     for (auto &d : rings) need_w |= (d.mode == kBluestein);
     if (need_w) {
