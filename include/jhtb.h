@@ -42,7 +42,10 @@ extern "C" {
 /* Arithmetic used by the contraction.  The recursion, seeds, coefficients and
  * the ring FFTs are FP64 in every mode. */
 #define JHTB_PREC_FP64 0 /* plain FP64 everywhere */
-#define JHTB_PREC_FP32 1 /* FP32 contraction, FP32 accumulation */
+#define JHTB_PREC_FP32 1 /* FP32 contraction, FP32 accumulation (not available yet) */
+#define JHTB_PREC_BF16X3 2 /* batched: mu and a_lm rounded to FP32 and split into three BF16
+                              parts; six split products per tile on the tensor cores (tcgen05),
+                              FP32 accumulation folded into FP64 every 64 l */
 
 typedef struct jhtb_plan jhtb_plan;
 
@@ -140,6 +143,10 @@ int jhtb_plan_set_timing(jhtb_plan *plan, int enable);
 /* Sum of recorded stage times (ms[4], milliseconds) and launch counts (counts[4]);
  * waits for the recorded events.  reset != 0 drops the records. */
 int jhtb_plan_timings(jhtb_plan *plan, double *ms, int64_t *counts, int reset);
+
+/* Device-side error status of the plan's kernels (0 = none, 1 = a bounded wait in a
+ * tensor-core kernel timed out).  Synchronises the device to read it; resets it. */
+int jhtb_plan_status(jhtb_plan *plan, int *device_error);
 
 /* FP64 FMA throughput probe: a grid of 148*blocks_per_sm CTAs x 256 threads, each
  * running 8 independent FMA chains for `iters` steps.  Writes the elapsed time of

@@ -23,7 +23,7 @@ JHTB_ERR_UNSUPPORTED = -2
 JHTB_ERR_CUDA = -3
 JHTB_ERR_NOMEM = -4
 
-PRECISIONS = {"fp64": 0, "fp32": 1}
+PRECISIONS = {"fp64": 0, "fp32": 1, "bf16x3": 2}
 
 # every exported symbol of include/jhtb.h (checked by the CPU test suite)
 EXPORTS = (
@@ -41,6 +41,7 @@ EXPORTS = (
     "jhtb_plan_timings",
     "jhtb_probe_fp64_fma",
     "jhtb_synthesis_noalloc",
+    "jhtb_plan_status",
 )
 
 
@@ -68,7 +69,8 @@ def load_library(path: str | os.PathLike | None = None):
     with _lib_lock:
         if _lib is not None and path is None:
             return _lib
-        p = Path(path) if path else LIB_PATH
+        env = os.environ.get("JHTB_LIBRARY")
+        p = Path(path) if path else (Path(env) if env else LIB_PATH)
         if not p.exists():
             raise ImportError(
                 f"jht_b200 CUDA library not found at {p}; build it with `python -m jht_b200.build` "
@@ -92,6 +94,7 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_probe_fp64_fma": (i32, [i32, i32, dp, ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double), vp]),
             "jhtb_synthesis_noalloc": (i32, [i32, i32, vp, vp, vp]),
+            "jhtb_plan_status": (i32, [vp, ctypes.POINTER(i32)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -194,6 +197,12 @@ class Plan:
         b = ctypes.c_int64()
         check(self.lib.jhtb_plan_bytes(self.handle, ctypes.byref(b)), "jhtb_plan_bytes")
         return int(b.value)
+
+    def status(self) -> int:
+        """Device error flag of the plan's kernels (synchronises); 0 = ok."""
+        e = ctypes.c_int()
+        check(self.lib.jhtb_plan_status(self.handle, ctypes.byref(e)), "jhtb_plan_status")
+        return int(e.value)
 
     def set_timing(self, enable: bool) -> None:
         check(self.lib.jhtb_plan_set_timing(self.handle, int(enable)), "jhtb_plan_set_timing")

@@ -36,8 +36,15 @@ constexpr double kLogScaleLo = 3.85953392016288e-10;  // 800 ln 2 - kLogScaleHi
 constexpr double kLn2x400 = 277.25887222397812;       // 400 ln 2
 
 // Legendre kernels: half-grid rings per lane (a warp tile is 32 * R consecutive rings).
-constexpr int kR0 = 4;  // spin 0
-constexpr int kR2 = 2;  // spin 2
+#ifndef JHTB_R0
+#define JHTB_R0 4
+#endif
+#ifndef JHTB_R2
+#define JHTB_R2 2
+#endif
+constexpr int kR0 = JHTB_R0;  // spin 0
+constexpr int kR2 = JHTB_R2;  // spin 2
+constexpr int kTcMaps = 8;    // maps per tensor-core pass (N = 4 * maps per GEMM)
 
 // FFT: largest power-of-two length handled in one CTA's shared memory.
 constexpr int kFftMax = 8192;
@@ -107,6 +114,15 @@ struct Plan {
     unsigned *d_counter; // work-queue counter
     double2 *d_part;     // [chunk][nsuper][ncomp][K] adjoint partial sums
 
+    // tensor-core path (precision BF16X3): 128-ring tiles (start tables built with R = 4)
+    int tc_ntiles;
+    int *d_tc_lw;
+    double2 *d_tc_st;
+    int *d_tc_stsc;
+    int *d_tc_order;
+    bool tc_owns_tables;  // false when they alias the FP64 tables (spin 0, R0 = 4)
+    int *d_err;           // device error flag
+
     // workspace
     double2 *d_F;       // [chunk][nchan][nrings][M] ring spectra
     double2 *d_W;       // [chunk][npix] Bluestein accumulation scratch (adjoint, Q > 1)
@@ -132,6 +148,8 @@ int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cud
 int launch_ring_adjoint(const Plan &p, const double *maps, double2 *F, double2 *W, int nb,
                         cudaStream_t s);
 int launch_start_states(const Plan &p, cudaStream_t s);
+int launch_start_states_r(const Plan &p, int R, int ntiles, int *lw, double2 *st, int *stsc, cudaStream_t s);
+int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaStream_t s);
 int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *offs, int nlen,
                            cudaStream_t s);
 

@@ -43,7 +43,10 @@ namespace {
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kStage = 32;  // steps staged per warp per round (one per lane)
-constexpr int kSub = 8;     // adjoint steps per warp reduction
+#ifndef JHTB_ADJ_SUB
+#define JHTB_ADJ_SUB 8
+#endif
+constexpr int kSub = JHTB_ADJ_SUB;  // adjoint steps per warp reduction
 constexpr unsigned kFull = 0xffffffffu;
 
 struct LegParams {
@@ -246,7 +249,7 @@ struct Stage0 {
     double2 c[kStage];
 };
 struct Stage2 {
-    double al[kStage], ga[kStage];
+    double2 ag[kStage];  // (alpha, gamma)
     double2 cp[kStage], cm[kStage];
 };
 
@@ -270,6 +273,14 @@ template <int R, bool SLOW>
 __device__ __forceinline__ void synth0_chunk(int cnt, const Stage0 &sb, const double (&x)[R], double (&u1)[R],
                                              double (&u2)[R], int (&sc)[R], double (&Ar)[R], double (&Ai)[R],
                                              double (&Br)[R], double (&Bi)[R]) {
+    if (cnt == kStage) {
+#pragma unroll
+        for (int q = 0; q < kStage; q += 2) {
+            synth0_step<R, SLOW>(sb.al[q], sb.c[q], x, u1, u2, sc, Ar, Ai);
+            synth0_step<R, SLOW>(sb.al[q + 1], sb.c[q + 1], x, u1, u2, sc, Br, Bi);
+        }
+        return;
+    }
     int q = 0;
     for (; q + 1 < cnt; q += 2) {
         synth0_step<R, SLOW>(sb.al[q], sb.c[q], x, u1, u2, sc, Ar, Ai);
@@ -385,12 +396,20 @@ template <int R, bool SLOW>
 __device__ __forceinline__ void synth2_chunk(int cnt, const Stage2 &sb, const double (&x)[R], double (&p1)[R],
                                              double (&p2)[R], int (&sp)[R], double (&m1)[R], double (&m2)[R],
                                              int (&sm)[R], Acc2 (&acc)[R]) {
+    if (cnt == kStage) {  // whole chunk: fully unrolled so the shared-memory loads pipeline
+#pragma unroll
+        for (int q = 0; q < kStage; q += 2) {
+            synth2_step<R, SLOW, 1>(sb.ag[q].x, sb.ag[q].y, sb.cp[q], sb.cm[q], x, p1, p2, sp, m1, m2, sm, acc);
+            synth2_step<R, SLOW, -1>(sb.ag[q + 1].x, sb.ag[q + 1].y, sb.cp[q + 1], sb.cm[q + 1], x, p1, p2, sp, m1, m2, sm, acc);
+        }
+        return;
+    }
     int q = 0;
     for (; q + 1 < cnt; q += 2) {
-        synth2_step<R, SLOW, 1>(sb.al[q], sb.ga[q], sb.cp[q], sb.cm[q], x, p1, p2, sp, m1, m2, sm, acc);
-        synth2_step<R, SLOW, -1>(sb.al[q + 1], sb.ga[q + 1], sb.cp[q + 1], sb.cm[q + 1], x, p1, p2, sp, m1, m2, sm, acc);
+        synth2_step<R, SLOW, 1>(sb.ag[q].x, sb.ag[q].y, sb.cp[q], sb.cm[q], x, p1, p2, sp, m1, m2, sm, acc);
+        synth2_step<R, SLOW, -1>(sb.ag[q + 1].x, sb.ag[q + 1].y, sb.cp[q + 1], sb.cm[q + 1], x, p1, p2, sp, m1, m2, sm, acc);
     }
-    if (q < cnt) synth2_step<R, SLOW, 1>(sb.al[q], sb.ga[q], sb.cp[q], sb.cm[q], x, p1, p2, sp, m1, m2, sm, acc);
+    if (q < cnt) synth2_step<R, SLOW, 1>(sb.ag[q].x, sb.ag[q].y, sb.cp[q], sb.cm[q], x, p1, p2, sp, m1, m2, sm, acc);
 }
 
 template <int R>
@@ -436,8 +455,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth2_kernel(LegParams p
                 const long long idx = b0 + i0 + lane;
                 const double c = p.cnorm[idx];
                 const double2 e = aE[idx], bb = aB[idx];
-                sb.al[lane] = p.alpha[idx];
-                sb.ga[lane] = p.gamma[idx];
+                sb.ag[lane] = make_double2(p.alpha[idx], p.gamma[idx]);
                 // cp = -(aE + i aB) c, cm = -(aE - i aB) c   (healpix.py:316-318)
                 sb.cp[lane] = make_double2(-(e.x - bb.y) * c, -(e.y + bb.x) * c);
                 sb.cm[lane] = make_double2(-(e.x + bb.y) * c, -(e.y - bb.x) * c);
@@ -505,19 +523,19 @@ __device__ __forceinline__ int scatter_index(int lane) {
 
 template <int NV>
 __device__ __forceinline__ bool scatter_writer(int lane) {
-    constexpr int used = NV == 8 ? 3 : (NV == 16 ? 4 : 5);
+    constexpr int used = NV == 4 ? 2 : (NV == 8 ? 3 : (NV == 16 ? 4 : 5));
     return (lane & ((1 << (5 - used)) - 1)) == 0;
 }
 
 struct AStage {
-    double al[kStage], ga[kStage];
+    double2 ag[kStage];  // (alpha, gamma)
 };
 
 // ---------------- spin 0 ----------------
 template <int R, bool SLOW>
 __device__ __forceinline__ double2 adj0_step(double al, const double (&x)[R], double (&u1)[R], double (&u2)[R],
                                              int (&sc)[R], const double2 (&U)[R]) {
-    double2 part[R];
+    double2 part = make_double2(0.0, 0.0);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         double u = fma(al * x[k], u1[k], -u2[k]);
@@ -526,16 +544,10 @@ __device__ __forceinline__ double2 adj0_step(double al, const double (&x)[R], do
         u2[k] = prev;
         u1[k] = u;
         if (SLOW && sc[k] != 0) u = 0.0;
-        part[k] = make_double2(u * U[k].x, u * U[k].y);
+        part.x = fma(u, U[k].x, part.x);
+        part.y = fma(u, U[k].y, part.y);
     }
-#pragma unroll
-    for (int s = 1; s < R; s *= 2)
-#pragma unroll
-        for (int k = 0; k + s < R; k += 2 * s) {
-            part[k].x += part[k + s].x;
-            part[k].y += part[k + s].y;
-        }
-    return part[0];
+    return part;
 }
 
 template <int R>
@@ -589,20 +601,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj0_kernel(LegParams p, 
             }
             for (int i0 = i_start; i0 < nst; i0 += kStage) {
                 const int cnt = min(kStage, nst - i0);
-                if (lane < cnt) sb.al[lane] = p.alpha[b0 + i0 + lane];
+                if (lane < cnt) sb.ag[lane].x = p.alpha[b0 + i0 + lane];
                 __syncwarp();
                 for (int q0 = 0; q0 < cnt; q0 += kSub) {
                     double2 v[kSub];
+                    // the writer lane's output slot is known up front: issue its load of
+                    // the running row sum now so the L2 round trip overlaps the steps
+                    const int qw = q0 + scatter_index<kSub>(lane);
+                    const bool wr = scatter_writer<kSub>(lane) && qw < cnt;
+                    double2 prev = make_double2(0.0, 0.0);
+                    if (acc && wr) prev = part[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
 #pragma unroll
                     for (int q = 0; q < kSub; q += 2) {
                         if (q0 + q < cnt)
-                            v[q] = f ? adj0_step<R, false>(sb.al[q0 + q], x, u1, u2, sc, UA)
-                                     : adj0_step<R, true>(sb.al[q0 + q], x, u1, u2, sc, UA);
+                            v[q] = f ? adj0_step<R, false>(sb.ag[q0 + q].x, x, u1, u2, sc, UA)
+                                     : adj0_step<R, true>(sb.ag[q0 + q].x, x, u1, u2, sc, UA);
                         else v[q] = make_double2(0.0, 0.0);
                         if (q0 + q + 1 < cnt)
-                            v[q + 1] = f ? adj0_step<R, false>(sb.al[q0 + q + 1], x, u1, u2, sc, UB)
-                                         : adj0_step<R, true>(sb.al[q0 + q + 1], x, u1, u2, sc, UB);
+                            v[q + 1] = f ? adj0_step<R, false>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB)
+                                         : adj0_step<R, true>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB);
                         else v[q + 1] = make_double2(0.0, 0.0);
                     }
                     if (!f) {
@@ -611,17 +629,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj0_kernel(LegParams p, 
                         for (int r = 0; r < R; ++r) fast &= sc[r] == 0;
                     }
                     warp_reduce_scatter<kSub>(v, lane);
-                    const int q = q0 + scatter_index<kSub>(lane);
-                    if (scatter_writer<kSub>(lane) && q < cnt) {
-                        const long long idx = b0 + i0 + q;
-                        double2 o = v[0];
-                        if (acc) {
-                            const double2 prev = part[idx];
-                            o.x += prev.x;
-                            o.y += prev.y;
-                        }
-                        part[idx] = o;
-                    }
+                    if (wr) part[b0 + i0 + qw] = make_double2(v[0].x + prev.x, v[0].y + prev.y);
                 }
                 __syncwarp();
             }
@@ -641,7 +649,8 @@ template <int R, bool SLOW, int SGN>
 __device__ __forceinline__ void adj2_step(double al, double ga, const double (&x)[R], double (&p1)[R],
                                           double (&p2)[R], int (&sp)[R], double (&m1)[R], double (&m2)[R],
                                           int (&sm)[R], const In2 (&in)[R], double2 &op, double2 &om) {
-    double2 pp[R], pm[R];
+    op = make_double2(0.0, 0.0);
+    om = make_double2(0.0, 0.0);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const double tp = fma(al, x[k], ga);
@@ -663,20 +672,15 @@ __device__ __forceinline__ void adj2_step(double al, double ga, const double (&x
         }
         const In2 &d = in[k];
         // p2 += lp Vpn + (-1)^l lm Sp ;  m2 += lm Vmn + (-1)^l lp Sm   (_recursion.py:565-566)
-        pp[k] = make_double2(fma(up, d.vpn.x, SGN * um * d.spA.x), fma(up, d.vpn.y, SGN * um * d.spA.y));
-        pm[k] = make_double2(fma(um, d.vmn.x, SGN * up * d.smA.x), fma(um, d.vmn.y, SGN * up * d.smA.y));
+        op.x = fma(up, d.vpn.x, op.x);
+        op.y = fma(up, d.vpn.y, op.y);
+        om.x = fma(um, d.vmn.x, om.x);
+        om.y = fma(um, d.vmn.y, om.y);
+        op.x = fma(SGN * um, d.spA.x, op.x);
+        op.y = fma(SGN * um, d.spA.y, op.y);
+        om.x = fma(SGN * up, d.smA.x, om.x);
+        om.y = fma(SGN * up, d.smA.y, om.y);
     }
-#pragma unroll
-    for (int s = 1; s < R; s *= 2)
-#pragma unroll
-        for (int k = 0; k + s < R; k += 2 * s) {
-            pp[k].x += pp[k + s].x;
-            pp[k].y += pp[k + s].y;
-            pm[k].x += pm[k + s].x;
-            pm[k].y += pm[k + s].y;
-        }
-    op = pp[0];
-    om = pm[0];
 }
 
 template <int R>
@@ -743,25 +747,28 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj2_kernel(LegParams p, 
             }
             for (int i0 = i_start; i0 < nst; i0 += kStage) {
                 const int cnt = min(kStage, nst - i0);
-                if (lane < cnt) {
-                    sb.al[lane] = p.alpha[b0 + i0 + lane];
-                    sb.ga[lane] = p.gamma[b0 + i0 + lane];
-                }
+                if (lane < cnt) sb.ag[lane] = make_double2(p.alpha[b0 + i0 + lane], p.gamma[b0 + i0 + lane]);
                 __syncwarp();
                 for (int q0 = 0; q0 < cnt; q0 += kSub) {
                     double2 v[NV];
+                    const int e = scatter_index<NV>(lane);  // 0..kSub-1: p2, kSub..: m2
+                    const int qw = q0 + (e & (kSub - 1));
+                    const bool wr = scatter_writer<NV>(lane) && qw < cnt;
+                    double2 *dstw = e >= kSub ? partM : partP;
+                    double2 prev = make_double2(0.0, 0.0);
+                    if (acc && wr) prev = dstw[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
 #pragma unroll
                     for (int q = 0; q < kSub; q += 2) {
                         if (q0 + q < cnt) {
-                            if (f) adj2_step<R, false, 1>(sb.al[q0 + q], sb.ga[q0 + q], x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
-                            else adj2_step<R, true, 1>(sb.al[q0 + q], sb.ga[q0 + q], x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
+                            if (f) adj2_step<R, false, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
+                            else adj2_step<R, true, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
                         } else {
                             v[q] = v[kSub + q] = make_double2(0.0, 0.0);
                         }
                         if (q0 + q + 1 < cnt) {
-                            if (f) adj2_step<R, false, -1>(sb.al[q0 + q + 1], sb.ga[q0 + q + 1], x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
-                            else adj2_step<R, true, -1>(sb.al[q0 + q + 1], sb.ga[q0 + q + 1], x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
+                            if (f) adj2_step<R, false, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
+                            else adj2_step<R, true, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
                         } else {
                             v[q + 1] = v[kSub + q + 1] = make_double2(0.0, 0.0);
                         }
@@ -772,21 +779,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj2_kernel(LegParams p, 
                         for (int r = 0; r < R; ++r) fast &= (sp[r] == 0) && (sm[r] == 0);
                     }
                     warp_reduce_scatter<NV>(v, lane);
-                    if (scatter_writer<NV>(lane)) {
-                        const int e = scatter_index<NV>(lane);  // 0..7: p2, 8..15: m2
-                        const int q = q0 + (e & (kSub - 1));
-                        if (q < cnt) {
-                            double2 *dst = e >= kSub ? partM : partP;
-                            const long long idx = b0 + i0 + q;
-                            double2 o = v[0];
-                            if (acc) {
-                                const double2 prev = dst[idx];
-                                o.x += prev.x;
-                                o.y += prev.y;
-                            }
-                            dst[idx] = o;
-                        }
-                    }
+                    if (wr) dstw[b0 + i0 + qw] = make_double2(v[0].x + prev.x, v[0].y + prev.y);
                 }
                 __syncwarp();
             }
@@ -868,6 +861,22 @@ int launch_start_states(const Plan &p, cudaStream_t s) {
     LegParams q = make_params(p);
     if (p.spin == 0) start_state_kernel<0, kR0><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
     else start_state_kernel<2, kR2><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
+    JHTB_CUDA_TRY(cudaGetLastError());
+    return JHTB_OK;
+}
+
+int launch_start_states_r(const Plan &p, int R, int ntiles, int *lw, double2 *st, int *stsc, cudaStream_t s) {
+    const int nitems = p.M * ntiles;
+    const int grid = (nitems + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    LegParams q = make_params(p);
+    q.ntiles = ntiles;
+    q.lw = lw;
+    q.st = st;
+    q.stsc = stsc;
+    if (p.spin == 0 && R == 4) start_state_kernel<0, 4><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
+    else if (p.spin == 2 && R == 4) start_state_kernel<2, 4><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
+    else if (p.spin == 2 && R == 2) start_state_kernel<2, 2><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
+    else return fail(JHTB_ERR_UNSUPPORTED, "start states: unsupported tile width");
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
 }

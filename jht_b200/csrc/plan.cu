@@ -86,9 +86,14 @@ void free_plan(Plan *p) {
     void *ptrs[] = {p->d_x,     p->d_logsin, p->d_logch, p->d_logsh,   p->d_rings, p->d_tw,
                     p->d_bh,    p->d_seed,   p->d_alpha, p->d_gamma,   p->d_cnorm, p->d_F,
                     p->d_W,     p->d_scratch, p->d_lw, p->d_st, p->d_stsc, p->d_synth_order,
-                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part};
+                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    if (p->tc_owns_tables) {
+        void *tc[] = {p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, p->d_tc_order};
+        for (void *q : tc)
+            if (q) cudaFree(q);
+    }
     for (auto &e : p->events) {
         cudaEventDestroy(e.start);
         cudaEventDestroy(e.stop);
@@ -253,6 +258,38 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         if ((rc = upload(&p->d_adj_tiles, at, bytes))) return rc;
     }
 
+    // ---- tensor-core path: 128-ring tiles ---------------------------------------------------
+    JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_err, sizeof(int)));
+    JHTB_CUDA_TRY(cudaMemset(p->d_err, 0, sizeof(int)));
+    if (p->precision == JHTB_PREC_BF16X3) {
+        const int Rt = 4;
+        if (spin == 0 && kR0 == Rt) {
+            p->tc_ntiles = p->ntiles;
+            p->d_tc_lw = p->d_lw;
+            p->d_tc_st = p->d_st;
+            p->d_tc_stsc = p->d_stsc;
+            p->d_tc_order = p->d_synth_order;
+            p->tc_owns_tables = false;
+        } else {
+            const int nrec = spin ? 2 : 1;
+            p->tc_ntiles = (T + 32 * Rt - 1) / (32 * Rt);
+            const long long nitems = (long long)M * p->tc_ntiles;
+            const size_t nel = (size_t)nitems * nrec * Rt * 32;
+            p->tc_owns_tables = true;
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_lw, sizeof(int) * nitems));
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_st, sizeof(double2) * nel));
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_stsc, sizeof(int) * nel));
+            bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nel;
+            if ((rc = launch_start_states_r(*p, Rt, p->tc_ntiles, p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, 0))) return rc;
+            JHTB_CUDA_TRY(cudaDeviceSynchronize());
+            std::vector<int> lw(nitems), so(nitems);
+            JHTB_CUDA_TRY(cudaMemcpy(lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
+            for (long long i = 0; i < nitems; ++i) so[i] = (int)i;
+            std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return lw[a] < lw[b]; });
+            if ((rc = upload(&p->d_tc_order, so, bytes))) return rc;
+        }
+    }
+
     // ---- ring FFT descriptors -------------------------------------------------------------
     std::vector<RingDesc> rings(nr);
     std::map<long long, long long> bh_offset;  // Bluestein length -> offset
@@ -385,7 +422,7 @@ int jhtb_plan_create(int nside, int lmax, int spin, int precision, int max_batch
     if (lmax < 0 || lmax > 16383) return fail(JHTB_ERR_INVALID, "lmax must be in [0, 16383]");
     if (precision == JHTB_PREC_FP32)
         return fail(JHTB_ERR_UNSUPPORTED, "FP32 contraction is not available in this build");
-    if (precision != JHTB_PREC_FP64)
+    if (precision != JHTB_PREC_FP64 && precision != JHTB_PREC_BF16X3)
         return fail(JHTB_ERR_INVALID, "unknown precision " + std::to_string(precision));
     if (max_batch < 1) return fail(JHTB_ERR_INVALID, "max_batch must be >= 1");
     Plan *p = new (std::nothrow) Plan();  // value-initialised: pointers null, counters zero
@@ -434,7 +471,8 @@ int jhtb_synthesis(jhtb_plan *plan, const void *alm, void *maps, int batch, void
         int rc;
         {
             StageTimer t(p, s, kStageLegSynth);
-            rc = launch_legendre_synth(p, a + (size_t)b0 * p.ncomp * p.K, p.d_F, nb, s);
+            rc = p.precision == JHTB_PREC_BF16X3 ? launch_tc_synth(p, a + (size_t)b0 * p.ncomp * p.K, p.d_F, nb, s)
+                                                 : launch_legendre_synth(p, a + (size_t)b0 * p.ncomp * p.K, p.d_F, nb, s);
         }
         if (rc) return rc;
         {
@@ -467,6 +505,15 @@ int jhtb_adjoint_synthesis(jhtb_plan *plan, const void *maps, void *alm, int bat
         }
         if (rc) return rc;
     }
+    return JHTB_OK;
+}
+
+int jhtb_plan_status(jhtb_plan *plan, int *device_error) {
+    if (!plan || !device_error) return fail(JHTB_ERR_INVALID, "jhtb_plan_status: NULL argument");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    JHTB_CUDA_TRY(cudaDeviceSynchronize());
+    JHTB_CUDA_TRY(cudaMemcpy(device_error, p.d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    JHTB_CUDA_TRY(cudaMemset(p.d_err, 0, sizeof(int)));
     return JHTB_OK;
 }
 
