@@ -1,0 +1,189 @@
+"""CPU-only checks of the boundary and the host-side logic (no GPU needed).
+
+* the C-ABI library loads and exports every function ``include/jhtb.h`` declares;
+* argument validation answers with a status code before any device work;
+* the host seed tables, ring geometry, packing, metric, quadrature weights and the
+  real-DOF isometry of the product package agree with the oracle and the golden
+  vectors produced by the reference's own code;
+* without a CUDA device the transforms raise instead of falling back to the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import ROOT, relerr
+
+import jht_b200 as jhtb  # noqa: E402
+from jht_b200 import _lib, healpix, masked, weights  # noqa: E402
+from oracle import jht_oracle as O  # noqa: E402
+
+HEADER = ROOT / "include" / "jhtb.h"
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not _lib.LIB_PATH.exists():
+        # incremental in-tree build (nvcc cross-compiles without a GPU)
+        subprocess.run([sys.executable, "-m", "jht_b200.build"], cwd=ROOT, check=True)
+    return _lib.load_library()
+
+
+def _declared_functions() -> set[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    return set(re.findall(r"\b(jhtb_[a-z0-9_]+)\s*\(", text))
+
+
+def test_header_declares_exactly_the_binding_exports():
+    assert _declared_functions() == set(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol(lib):
+    raw = ctypes.CDLL(str(_lib.LIB_PATH))
+    for name in sorted(_declared_functions()):
+        assert hasattr(raw, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], capture_output=True, text=True, check=True)
+    dyn = {ln.split()[-1] for ln in out.stdout.splitlines() if ln.strip()}
+    assert _declared_functions() <= dyn
+    # nothing else named jhtb_* leaks out of the shared object
+    assert {s for s in dyn if s.startswith("jhtb_")} == _declared_functions()
+
+
+def test_version_and_last_error(lib):
+    assert lib.jhtb_version() == 100
+    assert lib.jhtb_last_error(None, 0) == _lib.JHTB_ERR_INVALID
+
+
+@pytest.mark.parametrize(
+    "args,status,needle",
+    [
+        ((16, 24, 1, 0, 1), _lib.JHTB_ERR_UNSUPPORTED, "spin"),
+        ((0, 24, 0, 0, 1), _lib.JHTB_ERR_INVALID, "nside"),
+        ((8192, 24, 0, 0, 1), _lib.JHTB_ERR_INVALID, "nside"),
+        ((16, -1, 0, 0, 1), _lib.JHTB_ERR_INVALID, "lmax"),
+        ((16, 24, 0, 1, 1), _lib.JHTB_ERR_UNSUPPORTED, "FP32"),
+        ((16, 24, 0, 7, 1), _lib.JHTB_ERR_INVALID, "precision"),
+        ((16, 24, 0, 0, 0), _lib.JHTB_ERR_INVALID, "max_batch"),
+    ],
+)
+def test_plan_create_validates_before_device_work(lib, args, status, needle):
+    h = ctypes.c_void_p()
+    assert lib.jhtb_plan_create(*args, None, ctypes.byref(h)) == status
+    assert h.value is None
+    assert needle in _lib.last_error()
+
+
+def test_null_pointers_are_rejected(lib):
+    assert lib.jhtb_plan_create(16, 24, 0, 0, 1, None, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_synthesis(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_adjoint_synthesis(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_plan_destroy(None) == _lib.JHTB_OK
+
+
+@pytest.mark.parametrize("nside", [1, 4, 13, 64])
+def test_geometry_matches_oracle(nside):
+    g = healpix.RingInfo(nside)
+    r = O.Rings(nside)
+    np.testing.assert_array_equal(g.npix_ring, r.nring)
+    np.testing.assert_array_equal(g.startpix, r.start)
+    np.testing.assert_allclose(g.z, r.z, rtol=0, atol=0)
+    np.testing.assert_allclose(g.phi0, r.phi0, rtol=0, atol=0)
+    np.testing.assert_array_equal(_lib._half_grid_z(nside), r.z[: 2 * nside])
+
+
+@pytest.mark.parametrize("lmax", [0, 1, 7, 100])
+def test_packing_and_metric(lmax):
+    assert jhtb.alm_size(lmax) == O.alm_size(lmax)
+    for m in range(lmax + 1):
+        assert healpix.alm_column_base(m, lmax) == O.alm_base(m, lmax)
+    np.testing.assert_array_equal(jhtb.alm_metric_weight(lmax), O.metric_weight(lmax))
+
+
+@pytest.mark.parametrize("nside,lmax", [(8, 12), (16, 40), (64, 128)])
+def test_host_seed_tables_match_oracle(nside, lmax):
+    t0 = _lib.host_tables(nside, lmax, 0)
+    for m in range(lmax + 1):
+        assert abs(t0["seed_logc"][m] - O.sectoral_log_const(m)) <= 1e-13 * max(1.0, abs(O.sectoral_log_const(m)))
+    t2 = _lib.host_tables(nside, lmax, 2)
+    for h, s in enumerate((2, -2)):
+        for m in range(lmax + 1):
+            lmin = max(m, 2)
+            # at x = 0 both half-angle factors are sqrt(1/2) and their powers sum to 2 lmin
+            _, logd = O.wigner_seed(np.zeros(1), -m, s, lmin)
+            logc = float(logd[0]) + lmin * np.log(2.0)
+            assert abs(t2["seed_logc"][h, m] - logc) <= 1e-12 * max(1.0, abs(logc)), (s, m)
+
+
+@pytest.mark.parametrize("nside", [1, 2, 4, 8, 12, 16, 32, 64])
+def test_ring_weights_match_golden(golden, nside):
+    np.testing.assert_allclose(weights.ring_weights(nside), golden[f"weights/ring_n{nside}"], rtol=0, atol=1e-12)
+
+
+def test_pixel_weights_match_golden(golden):
+    np.testing.assert_allclose(weights.pixel_weights(8), golden["weights/pix_n8"], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(weights.pixel_weights(8, False), np.full(768, 4 * np.pi / 768), rtol=1e-15)
+
+
+def test_real_dof_matches_golden_on_cpu(golden):
+    x0 = masked.alm_to_real(torch.as_tensor(golden["real/a0"]), 12, 0)
+    x2 = masked.alm_to_real(torch.as_tensor(golden["real/a2"]), 12, 2)
+    np.testing.assert_array_equal(x0.numpy(), golden["real/x0"])
+    np.testing.assert_array_equal(x2.numpy(), golden["real/x2"])
+    np.testing.assert_allclose(masked.real_to_alm(x0, 12, 0).numpy(), golden["real/a0"], atol=1e-15)
+    np.testing.assert_allclose(masked.real_to_alm(x2, 12, 2).numpy(), golden["real/a2"], atol=1e-15)
+    assert jhtb.n_dof(12, 0) == golden["real/x0"].size
+    assert jhtb.n_dof(12, 2) == golden["real/x2"].size
+
+
+@pytest.mark.parametrize("lmax,spin", [(0, 0), (5, 0), (30, 0), (5, 2), (30, 2)])
+def test_real_dof_is_an_isometry(lmax, spin):
+    rng = np.random.default_rng(lmax + spin)
+    n = jhtb.n_dof(lmax, spin)
+    x = torch.as_tensor(rng.standard_normal(n))
+    a = masked.real_to_alm(x, lmax, spin)
+    back = masked.alm_to_real(a, lmax, spin)
+    np.testing.assert_allclose(back.numpy(), x.numpy(), rtol=0, atol=1e-15)
+    G = torch.as_tensor(jhtb.alm_metric_weight(lmax))
+    na = float(torch.sum(G * a.abs() ** 2))
+    assert abs(na - float(torch.sum(x * x))) <= 1e-12 * max(1.0, na)
+    # batch helpers used by the CG agree with the single-vector form
+    xb = torch.stack([x, 2 * x])
+    ab = masked._alm_batch(xb, lmax, spin)
+    np.testing.assert_allclose(ab[0].reshape(a.shape).numpy(), a.numpy(), atol=0)
+    np.testing.assert_allclose(masked._real_batch(ab, lmax, spin).numpy(), xb.numpy(), atol=1e-15)
+
+
+def test_bandpower_matches_oracle():
+    rng = np.random.default_rng(3)
+    lmax = 20
+    K = jhtb.alm_size(lmax)
+    a = rng.standard_normal((2, K)) + 1j * rng.standard_normal((2, K))
+    got = jhtb.bandpower(torch.as_tensor(a), lmax, 2).numpy()
+    assert relerr(got, O.bandpower(a, lmax, 2)) <= 1e-14
+
+
+def test_workspace_budget_caps_batch():
+    per = _lib.workspace_bytes_per_map(2048, 4096, 2)
+    assert per > 1 << 30
+    assert _lib.workspace_bytes_per_map(64, 128, 0) < _lib.workspace_bytes_per_map(64, 128, 2)
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the behaviour on a host without CUDA")
+def test_no_cpu_fallback():
+    a = np.zeros(jhtb.alm_size(8), dtype=np.complex128)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        jhtb.synthesis(a, 8, 8, 0)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        jhtb.adjoint_synthesis(np.zeros(768), 8, 8, 0)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        jhtb.analysis(np.zeros(768), 8, 8, 0)
