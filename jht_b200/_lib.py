@@ -24,6 +24,7 @@ JHTB_ERR_CUDA = -3
 JHTB_ERR_NOMEM = -4
 
 PRECISIONS = {"fp64": 0, "fp32": 1, "bf16x3": 2}
+TC_MAPS = 8  # maps per tensor-core GEMM group (kTcMaps in the CUDA sources)
 
 # every exported symbol of include/jhtb.h (checked by the CPU test suite)
 EXPORTS = (
@@ -243,7 +244,15 @@ def get_plan(nside: int, lmax: int, spin: int, precision: str = "fp64", batch: i
 
     dev = torch.cuda.current_device()
     per = workspace_bytes_per_map(nside, lmax, spin)
-    cap = max(1, min(64, (4 << 30) // per))
+    if precision == "bf16x3":
+        # the tensor-core path shares one recursion among the maps of a pass: hold whole
+        # groups of TC_MAPS maps when device memory allows
+        free, _ = torch.cuda.mem_get_info(dev)
+        cap = max(1, min(64, min(32 << 30, free // 3) // per))
+        if cap >= TC_MAPS:
+            cap -= cap % TC_MAPS
+    else:
+        cap = max(1, min(64, (4 << 30) // per))
     want = max(1, min(batch, cap))
     key = (dev, nside, lmax, spin, precision)
     with _plans_lock:

@@ -120,7 +120,7 @@ struct Plan {
     double2 *d_tc_st;
     int *d_tc_stsc;
     int *d_tc_order;
-    bool tc_owns_tables;  // false when they alias the FP64 tables (spin 0, R0 = 4)
+    bool tc_owns_tables;
     int *d_err;           // device error flag
 
     // workspace

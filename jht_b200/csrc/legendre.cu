@@ -874,6 +874,7 @@ int launch_start_states_r(const Plan &p, int R, int ntiles, int *lw, double2 *st
     q.st = st;
     q.stsc = stsc;
     if (p.spin == 0 && R == 4) start_state_kernel<0, 4><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
+    else if (p.spin == 0 && R == 8) start_state_kernel<0, 8><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
     else if (p.spin == 2 && R == 4) start_state_kernel<2, 4><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
     else if (p.spin == 2 && R == 2) start_state_kernel<2, 2><<<grid, kWarpsPerBlock * 32, 0, s>>>(q, nitems);
     else return fail(JHTB_ERR_UNSUPPORTED, "start states: unsupported tile width");

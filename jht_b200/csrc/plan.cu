@@ -262,32 +262,25 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_err, sizeof(int)));
     JHTB_CUDA_TRY(cudaMemset(p->d_err, 0, sizeof(int)));
     if (p->precision == JHTB_PREC_BF16X3) {
-        const int Rt = 4;
-        if (spin == 0 && kR0 == Rt) {
-            p->tc_ntiles = p->ntiles;
-            p->d_tc_lw = p->d_lw;
-            p->d_tc_st = p->d_st;
-            p->d_tc_stsc = p->d_stsc;
-            p->d_tc_order = p->d_synth_order;
-            p->tc_owns_tables = false;
-        } else {
-            const int nrec = spin ? 2 : 1;
-            p->tc_ntiles = (T + 32 * Rt - 1) / (32 * Rt);
-            const long long nitems = (long long)M * p->tc_ntiles;
-            const size_t nel = (size_t)nitems * nrec * Rt * 32;
-            p->tc_owns_tables = true;
-            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_lw, sizeof(int) * nitems));
-            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_st, sizeof(double2) * nel));
-            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_stsc, sizeof(int) * nel));
-            bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nel;
-            if ((rc = launch_start_states_r(*p, Rt, p->tc_ntiles, p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, 0))) return rc;
-            JHTB_CUDA_TRY(cudaDeviceSynchronize());
-            std::vector<int> lw(nitems), so(nitems);
-            JHTB_CUDA_TRY(cudaMemcpy(lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
-            for (long long i = 0; i < nitems; ++i) so[i] = (int)i;
-            std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return lw[a] < lw[b]; });
-            if ((rc = upload(&p->d_tc_order, so, bytes))) return rc;
-        }
+        // tensor-core tiles: 128 rings x both recursions (spin 2) or 256 rings (spin 0),
+        // so each producer thread of the batched kernel runs two recursion chains
+        const int Rt = spin ? 4 : 8;
+        const int nrec = spin ? 2 : 1;
+        p->tc_ntiles = (T + 32 * Rt - 1) / (32 * Rt);
+        const long long nitems = (long long)M * p->tc_ntiles;
+        const size_t nel = (size_t)nitems * nrec * Rt * 32;
+        p->tc_owns_tables = true;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_lw, sizeof(int) * nitems));
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_st, sizeof(double2) * nel));
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_stsc, sizeof(int) * nel));
+        bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nel;
+        if ((rc = launch_start_states_r(*p, Rt, p->tc_ntiles, p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, 0))) return rc;
+        JHTB_CUDA_TRY(cudaDeviceSynchronize());
+        std::vector<int> lw(nitems), so(nitems);
+        JHTB_CUDA_TRY(cudaMemcpy(lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < nitems; ++i) so[i] = (int)i;
+        std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return lw[a] < lw[b]; });
+        if ((rc = upload(&p->d_tc_order, so, bytes))) return rc;
     }
 
     // ---- ring FFT descriptors -------------------------------------------------------------

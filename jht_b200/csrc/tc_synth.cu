@@ -5,19 +5,29 @@
 // n = (map, component) (N = 4 B per GEMM).  Spin 2 runs two GEMMs, one per
 // recursion (+2 / -2):  D+ = Lambda+ [cp, s cm],  D- = Lambda- [cm, s cp], with
 // s = (-1)^(l - lmin) folded into the B rows; jht's four half-grid sums
-// (_recursion.py:512-543) are the four column pairs.  Spin 0 runs one GEMM with
-// columns [a, s a] (_recursion.py:441-469).
+// (_recursion.py:512-543) are the four column pairs.  Spin 0 runs the same
+// contraction for two 128-ring halves of a 256-ring tile, columns [a, s a]
+// (_recursion.py:441-469).
 //
-// Each thread owns one ring: it runs the FP64 recursion (same normalised form and
-// start states as the FP64 kernels), rounds mu to FP32 and splits it into three BF16
-// parts, and writes its row of the A tiles (K-major, no swizzle) in shared memory.
-// The B tiles (a_lm times c_l, split the same way) are written by all threads.  One
-// thread issues the six split products hh, hm, mh, hl, lh, mm per GEMM
-// (kind::f16, BF16 x BF16 -> FP32 in tensor memory); a commit to an mbarrier frees
-// the double-buffered stage.  Every kFlush chunks the FP32 accumulators are read
-// (tcgen05.ld) into FP64 registers and restarted, so FP32 rounding accumulates over
-// at most 64 l.  Every wait is bounded; on timeout the kernel records an error,
-// releases its tensor memory and returns.
+// The CTA is warp-specialised and its roles meet only at mbarriers:
+//   producer warps (one thread per A row = tensor-memory lane, two recursion chains
+//     per thread) run the FP64 recursion (same normalised form and start states as
+//     the FP64 kernels), round mu to FP32, split it into three BF16 parts and store
+//     their rows of the A operands straight into tensor memory (tcgen05.st), so the
+//     six split products never re-read A through shared memory;
+//   builder warps (one thread per (l, map) of a chunk) load a_lm and c_l two chunks
+//     ahead into registers, form the B rows (c_l a_lm with the N/S sign pattern),
+//     split them the same way into shared memory, and stage the chunk's recursion
+//     coefficients;
+//   one MMA warp issues the six split products hh, hm, mh, hl, lh, mm per GEMM
+//     (kind::f16, A from tensor memory, B from shared memory, FP32 accumulators in
+//     tensor memory) and commits each stage back to its producers.
+// hh accumulates apart from the five smaller products (relative size <= 2^-8).
+// Every kFlush chunks (128 l) the producers fold the FP32 block sums into per-thread
+// double-float (hi, lo) accumulators in shared memory, so FP32 rounding acts on at
+// most 128 terms; the item's result is hi + lo in FP64.  Every wait is bounded; on
+// timeout the kernel records an error, every role leaves its loop, and tensor memory
+// is released after the last MMA has drained.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -30,8 +40,7 @@ namespace {
 
 constexpr int kTcRows = 128;     // = MMA M = rings per tile
 constexpr int kTcK = 16;         // l steps per chunk = MMA K (BF16)
-constexpr int kFlush = 4;        // chunks per FP32 accumulation block
-constexpr int kSuper = 8;        // chunks per staging pass (coefficients + B tiles); multiple of kFlush
+constexpr int kFlush = 8;        // chunks per FP32 accumulation block
 constexpr unsigned kWaitLimit = 1u << 26;
 
 // ---------------------------------------------------------------------------------
@@ -87,26 +96,47 @@ __device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t adesc, uint64
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
         : "memory");
 }
+// A operand from tensor memory (ts form), B from a shared-memory descriptor.
+__device__ __forceinline__ void umma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(
+            d_tmem),
+        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
 
-// 32 lanes x 32 consecutive FP32 columns -> 32 registers per thread (its own lane's row).
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
-        "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// 32 lanes x 8 consecutive 32-bit columns <-> 8 registers per thread (its own lane's row).
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+                 "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                 "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                 "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(a), "r"(b), "r"(c),
+                 "r"(d)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // Shared-memory descriptor, K-major, no swizzle: 8-row x 16-byte core matrices,
 // LBO = byte distance between the two 8-element K halves, SBO = between 8-row groups.
@@ -139,9 +169,6 @@ __device__ __forceinline__ void split3_bits(double xd, uint32_t &h, uint32_t &m,
     const float r2 = r1 - __uint_as_float(m);
     l = __float_as_uint(r2) & 0xFFFF0000u;
 }
-// two BF16 high halves -> one packed word (first value in the low half)
-__device__ __forceinline__ uint32_t pack_hi(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x7632); }
-
 // BF16 of FP32 value x by truncation (used for the B tiles, same split as split3_bits)
 __device__ __forceinline__ void split3(double xd, __nv_bfloat16 &h, __nv_bfloat16 &m, __nv_bfloat16 &l) {
     uint32_t hb, mb, lb;
@@ -160,39 +187,106 @@ __device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {
     }
 }
 
+// Two values at once, packed as BF16 pairs (x0's part in the low half) from the
+// truncation split of split3_bits; only the FP64 -> FP32 rounding uses the conversion
+// pipe, the rest is integer and FP32 arithmetic.
+__device__ __forceinline__ void split3_pair(double x0d, double x1d, uint32_t &h, uint32_t &m, uint32_t &l) {
+    uint32_t h0, m0, l0, h1, m1, l1;
+    split3_bits(x0d, h0, m0, l0);
+    split3_bits(x1d, h1, m1, l1);
+    h = __byte_perm(h0, h1, 0x7632);
+    m = __byte_perm(m0, m1, 0x7632);
+    l = __byte_perm(l0, l1, 0x7632);
+}
+
 struct TcParams {
     int lmax, T, nrings, M, nside;
     long long K;
     const double *x;
     const SeedParam *seed;
     const double *alpha, *gamma, *cnorm;
-    int ntiles;  // 128-ring tiles per m
+    int ntiles;  // item tiles per m (128 rings for spin 2, 256 for spin 0)
     const int *lw;
     const double2 *st;
     const int *stsc;
     const int *order;
-    unsigned *counter;
     int *err;
 };
 
 template <int SPIN, int BM>
-struct TcSmem {
-    static constexpr int NG = SPIN ? 2 : 1;
-    static constexpr int N = 4 * BM;
-    // per stage: A tiles [NG][3 splits][128 x 16 bf16], B tiles [NG][3][N x 16 bf16]
-    alignas(1024) unsigned char A[2][NG][3][kTcRows * kTcK * 2];
-    // B tiles for all kSuper chunks of a 128-step super-chunk, built in one pass
-    alignas(128) unsigned char B[kSuper][NG][3][N * kTcK * 2];
-    double2 coef[kSuper * kTcK];  // (alpha, gamma) for the super-chunk's steps
-    alignas(8) uint64_t mbar[2];
-    uint32_t taddr;
-    int err;
+struct TcCfg {
+    static constexpr int NG = 2;                    // GEMMs per chunk = recursion chains per producer thread
+    static constexpr int NBT = SPIN ? 2 : 1;        // B tiles per chunk (spin 0: both GEMMs share one)
+    static constexpr int N = 4 * BM;                // columns per GEMM
+    static constexpr int NPW = 4;                   // producer warps: one thread per A row (TMEM lane)
+    static constexpr int NBW = 4;                   // builder warps: one thread per (l, map) of a chunk
+    static constexpr int MMA_WARP = NPW + NBW;
+    static constexpr int NTHREADS = (NPW + NBW + 1) * 32;
+    static constexpr int NSA = 2;                   // A stages (in tensor memory)
+    static constexpr int NSB = 4;                   // B stages (with the chunk's coefficients)
+    static constexpr int BTILE = N * kTcK * 2;
+    static constexpr int ACOLS = kTcK / 2;          // tensor-memory columns of one A row (16 BF16)
+    // tensor memory: per GEMM hh and corr block sums, then the A stages
+    static constexpr int COL_A = NG * 2 * N;
+    static constexpr int NCOL = COL_A + NSA * NG * 3 * ACOLS;
+    static constexpr uint32_t TCOLS = NCOL <= 32 ? 32 : (NCOL <= 64 ? 64 : (NCOL <= 128 ? 128 : 256));
+    static_assert(NBW * 32 == kTcK * BM, "one builder thread per (l, map) of a chunk");
+    static_assert(NCOL <= 256, "tensor memory of two resident CTAs");
 };
 
-// One step of one recursion with the scaled-phase bookkeeping (SLOW) or without.
+template <int SPIN, int BM>
+struct TcSmem {
+    using C = TcCfg<SPIN, BM>;
+    alignas(1024) unsigned char B[C::NSB][C::NBT][3][C::BTILE];
+    double2 coef[C::NSB][kTcK];  // (alpha, gamma) of the chunk's 16 steps
+    // double-float accumulators, [hi/lo][GEMM][column][row]: a warp touches 32 consecutive words
+    float acc[2][C::NG][C::N][kTcRows];
+    alignas(8) uint64_t fullA[C::NSA], emptyA[C::NSA], fullB[C::NSB], emptyB[C::NSB];
+    uint64_t accFull, accEmpty, fin;
+    uint32_t taddr;
+    int fail;
+};
+
+// One (m, ring tile, map group) work item, as every role of the CTA derives it.
+struct TcItem {
+    int item, m, lmin, i_start, nst, nck, b_lo, b_cnt, tile;
+    long long b0;
+};
+
+// Item info from its id (the loads of lmin and lw are issued here and consumed later).
+__device__ __forceinline__ TcItem tc_item_of(const TcParams &p, int it, int item, int nitems, int nb, int bm) {
+    TcItem q;
+    const int g = it / nitems;
+    q.item = item;
+    q.m = item / p.ntiles;
+    q.tile = item - q.m * p.ntiles;
+    q.lmin = __ldg(&p.seed[q.m].lmin);
+    q.b0 = alm_index(q.lmin, q.m, p.lmax);
+    q.nst = p.lmax - q.lmin + 1;
+    q.i_start = __ldg(&p.lw[item]) - q.lmin;
+    q.nck = q.i_start < q.nst ? (q.nst - q.i_start + kTcK - 1) / kTcK : 0;
+    q.b_lo = g * bm;
+    q.b_cnt = min(bm, nb - q.b_lo);
+    return q;
+}
+__device__ __forceinline__ int tc_order(const TcParams &p, int it, int nitems, int total) {
+    return it < total ? __ldg(&p.order[it % nitems]) : 0;
+}
+__device__ __forceinline__ TcItem tc_item(const TcParams &p, int it, int nitems, int nb, int bm) {
+    return tc_item_of(p, it, __ldg(&p.order[it % nitems]), nitems, nb, bm);
+}
+
+__device__ __forceinline__ bool tc_failed(const int *f) { return *(volatile const int *)f != 0; }
+__device__ __forceinline__ void tc_fail(int *f, int *err) {
+    *(volatile int *)f = 1;
+    atomicExch(err, 1);
+}
+
+// One step of one recursion, t = alpha_l x + gamma_l precomputed, with the
+// scaled-phase bookkeeping (SLOW) or without.
 template <bool SLOW>
-__device__ __forceinline__ double tc_step(double al, double ga, double x, double &u1, double &u2, int &sc) {
-    double u = fma(fma(al, x, ga), u1, -u2);
+__device__ __forceinline__ double tc_step(double t, double &u1, double &u2, int &sc) {
+    double u = fma(t, u1, -u2);
     double prev = u1;
     if (SLOW) rescale(u, prev, sc);
     u2 = prev;
@@ -200,267 +294,444 @@ __device__ __forceinline__ double tc_step(double al, double ga, double x, double
     return (SLOW && sc != 0) ? 0.0 : u;
 }
 
-// 16 steps -> packed BF16 rows (pk[split][word]) of this thread's ring.
+// 16 steps of this thread's two recursion chains, split into BF16 parts and stored as
+// its row (= its tensor-memory lane) of the two GEMMs' three A operands: tA0 / tA1 are
+// the lane-offset tensor-memory addresses of the chains' split-0 operands, the splits
+// following at ACOLS columns apart.  Spin 2: chain 0 is the +2 recursion (+gamma),
+// chain 1 the -2 one (-gamma), same ring; spin 0: the chains are rings row and
+// 128 + row of the item tile (gamma = 0).  Past the end of the column the
+// coefficients are zero, which keeps the state bounded (u_k = -u_{k-2}) while the B
+// rows there are zero; rows past the last ring start from a zero state and stay zero.
+// Each half-chunk first loads its eight coefficient pairs and forms the multipliers
+// t = alpha x +- gamma, so only one FMA per step stays on the dependency chain.
 template <bool SLOW>
-__device__ __forceinline__ void tc_chunk(const double2 *coef, int ncnt, double x, double gsign, bool valid, double &u1,
-                                         double &u2, int &sc, uint32_t (&pk)[3][kTcK / 2]) {
+__device__ __forceinline__ void tc_chunk2(const double2 *coef, double x0, double x1, double (&u1)[2], double (&u2)[2],
+                                          int (&sc)[2], uint32_t tA0, uint32_t tA1) {
+    constexpr uint32_t AC = kTcK / 2;
 #pragma unroll
-    for (int q = 0; q < kTcK; q += 2) {
-        double v0 = 0.0, v1 = 0.0;
-        if (q < ncnt) {
-            const double2 ag = coef[q];
-            v0 = tc_step<SLOW>(ag.x, gsign * ag.y, x, u1, u2, sc);
+    for (int half = 0; half < 2; ++half) {
+        double t0[8], t1[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const double2 a = coef[half * 8 + k];
+            t0[k] = fma(a.x, x0, a.y);
+            t1[k] = fma(a.x, x1, -a.y);
         }
-        if (q + 1 < ncnt) {
-            const double2 ag = coef[q + 1];
-            v1 = tc_step<SLOW>(ag.x, gsign * ag.y, x, u1, u2, sc);
+        uint32_t pk[2][3][4];
+#pragma unroll
+        for (int q = 0; q < 8; q += 2) {
+            const double v00 = tc_step<SLOW>(t0[q], u1[0], u2[0], sc[0]);
+            const double v10 = tc_step<SLOW>(t1[q], u1[1], u2[1], sc[1]);
+            const double v01 = tc_step<SLOW>(t0[q + 1], u1[0], u2[0], sc[0]);
+            const double v11 = tc_step<SLOW>(t1[q + 1], u1[1], u2[1], sc[1]);
+            split3_pair(v00, v01, pk[0][0][q / 2], pk[0][1][q / 2], pk[0][2][q / 2]);
+            split3_pair(v10, v11, pk[1][0][q / 2], pk[1][1][q / 2], pk[1][2][q / 2]);
         }
-        if (!valid) v0 = v1 = 0.0;
-        uint32_t h0, m0, l0, h1, m1, l1;
-        split3_bits(v0, h0, m0, l0);
-        split3_bits(v1, h1, m1, l1);
-        pk[0][q / 2] = pack_hi(h0, h1);
-        pk[1][q / 2] = pack_hi(m0, m1);
-        pk[2][q / 2] = pack_hi(l0, l1);
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int sp = 0; sp < 3; ++sp)
+                tmem_st4((j ? tA1 : tA0) + sp * AC + half * 4, pk[j][sp][0], pk[j][sp][1], pk[j][sp][2], pk[j][sp][3]);
     }
 }
 
+// (hi, lo) += s in double-float: error-free two-sum of hi + s, then renormalise.
+__device__ __forceinline__ void df_add(float &hi, float &lo, float s) {
+    const float t = hi + s;
+    const float bp = t - hi;
+    const float e = (hi - (t - bp)) + (s - bp);
+    const float l2 = lo + e;
+    hi = t + l2;
+    lo = l2 - (hi - t);
+}
+
+// Rows of F for one (map, ring): north (healpix.py:250-253) and the signed south mirror.
+// Spin 2: GEMM + (H = 0) holds [FpN | FmS], GEMM - (H = 1) holds [FmN | FpS].
+template <int SPIN>
+__device__ __forceinline__ void tc_store_F(const TcParams &p, double2 *__restrict__ F_all, int b, int H, int t, int m,
+                                           int lmin, const double (&v)[4]) {
+    const size_t rs = (size_t)(4 * p.nside - 2 - t);
+    if (SPIN) {
+        const double ssign = ((m + lmin) & 1) ? -1.0 : 1.0;
+        double2 *Fp = F_all + (size_t)b * 2 * p.nrings * p.M;
+        double2 *Fm = Fp + (size_t)p.nrings * p.M;
+        double2 *Fn = H ? Fm : Fp, *Fs = H ? Fp : Fm;
+        Fn[(size_t)t * p.M + m] = make_double2(v[0], v[1]);
+        if (t < p.T - 1) Fs[rs * p.M + m] = make_double2(ssign * v[2], ssign * v[3]);
+    } else {
+        double2 *F = F_all + (size_t)b * p.nrings * p.M;
+        F[(size_t)t * p.M + m] = make_double2(v[0], v[1]);
+        if (t < p.T - 1) F[rs * p.M + m] = make_double2(v[2], v[3]);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// producer warps: recursion -> A tiles; block folds and the item's output
+// ---------------------------------------------------------------------------------
 template <int SPIN, int BM>
-__global__ void __launch_bounds__(kTcRows * (SPIN ? 2 : 1), SPIN ? 2 : 3) tc_synth_kernel(TcParams p, const double2 *__restrict__ alm_all,
-                                                                           double2 *__restrict__ F_all, int nb) {
-    using S = TcSmem<SPIN, BM>;
-    constexpr int NG = S::NG, N = S::N;
-    constexpr int NTH = kTcRows * NG;           // one thread per (ring, recursion)
-    constexpr int NCOL = 2 * NG * N;            // per GEMM: hh accumulator + correction accumulator
-    constexpr uint32_t TCOLS = NCOL <= 32 ? 32 : (NCOL <= 64 ? 64 : (NCOL <= 128 ? 128 : 256));
+__device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__restrict__ F_all, int nb,
+                            uint32_t tbase, int warp, int lane) {
+    using C = TcCfg<SPIN, BM>;
+    constexpr int N = C::N;
+    const int row = warp * 32 + lane;  // A row = TMEM lane
+    const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16);
+    float(&acc)[2][C::NG][N][kTcRows] = sm.acc;
+    const int nitems = p.M * p.ntiles;
+    const int total = nitems * ((nb + BM - 1) / BM);
+    const int stride = gridDim.x;
+    unsigned gc = 0, bk = 0;
+    bool ok = true;
+    // chain j's ring (spin 0: two 128-ring halves of the item tile) and start-state slot
+    auto ring_of = [&](int tile, int j) { return SPIN ? tile * kTcRows + row : tile * 2 * kTcRows + j * kTcRows + row; };
+    auto st_of = [&](int id, int j) { return ((size_t)id * 2 + j) * kTcRows + row; };
+    // the next item's id, lmin, lw and start states are loaded one item ahead, the
+    // order entry two items ahead
+    int it = blockIdx.x;
+    int id = tc_order(p, it, nitems, total);
+    int id_next = tc_order(p, it + stride, nitems, total);
+    int lmin = __ldg(&p.seed[id / p.ntiles].lmin), lwv = __ldg(&p.lw[id]);
+    double2 st[2];
+    int stsc[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        st[j] = p.st[st_of(id, j)];
+        stsc[j] = p.stsc[st_of(id, j)];
+    }
+    for (; it < total && ok; it += stride) {
+        if (tc_failed(&sm.fail)) break;
+        const int id_nn = tc_order(p, it + 2 * stride, nitems, total);
+        const int lmin_n = __ldg(&p.seed[id_next / p.ntiles].lmin), lw_n = __ldg(&p.lw[id_next]);
+        double2 st_n[2];
+        int stsc_n[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            st_n[j] = p.st[st_of(id_next, j)];
+            stsc_n[j] = p.stsc[st_of(id_next, j)];
+        }
+
+        const int m = id / p.ntiles, tile = id - m * p.ntiles;
+        const int t0 = ring_of(tile, 0), t1 = ring_of(tile, 1);
+        const double x0 = t0 < p.T ? __ldg(&p.x[t0]) : 0.0;
+        const double x1 = SPIN ? x0 : (t1 < p.T ? __ldg(&p.x[t1]) : 0.0);
+        const int nst = p.lmax - lmin + 1, i_start = lwv - lmin;
+        const int nck = i_start < nst ? (nst - i_start + kTcK - 1) / kTcK : 0;
+        double u1[2] = {st[0].x, st[1].x}, u2[2] = {st[0].y, st[1].y};
+        int sc[2] = {t0 < p.T ? stsc[0] : 0, t1 < p.T ? stsc[1] : 0};
+        bool fast = sc[0] == 0 && sc[1] == 0;
+        for (int c = 0; c < nck; ++c, ++gc) {
+            const int sA = gc % C::NSA, sB = gc % C::NSB;
+            if (!mbar_wait(&sm.fullB[sB], (gc / C::NSB) & 1u)) { ok = false; break; }
+            if (gc >= (unsigned)C::NSA && !mbar_wait(&sm.emptyA[sA], ((gc / C::NSA) - 1u) & 1u)) { ok = false; break; }
+            tc_fence_after();  // the stage's previous MMAs are complete before it is overwritten
+            const uint32_t tA0 = tl + (uint32_t)(C::COL_A + (sA * C::NG) * 3 * C::ACOLS);
+            const uint32_t tA1 = tA0 + 3 * C::ACOLS;
+            if (__all_sync(0xffffffffu, fast)) {
+                tc_chunk2<false>(sm.coef[sB], x0, x1, u1, u2, sc, tA0, tA1);
+            } else {
+                tc_chunk2<true>(sm.coef[sB], x0, x1, u1, u2, sc, tA0, tA1);
+                fast = sc[0] == 0 && sc[1] == 0;
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&sm.fullA[sA]);
+                mbar_arrive(&sm.emptyB[sB]);
+            }
+            const bool last = c == nck - 1;
+            if ((c % kFlush) == kFlush - 1 || last) {
+                if (!mbar_wait(&sm.accFull, bk & 1u)) { ok = false; break; }
+                tc_fence_after();
+                const bool first_block = c < kFlush;
+                const int b_lo = (it / nitems) * BM, b_cnt = min(BM, nb - b_lo);
+#pragma unroll 1
+                for (int piece = 0; piece < 2 * N / 8; ++piece) {
+                    const int j = piece / (N / 8), c0 = (piece % (N / 8)) * 8;
+                    const uint32_t tg = tl + (uint32_t)(j * 2 * N + c0);
+                    float hh[8], co[8];
+                    tmem_ld8(tg, hh);
+                    tmem_ld8(tg + N, co);
+                    float hi[8], lo[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const float sblk = hh[q] + co[q];
+                        if (first_block) {
+                            hi[q] = sblk;
+                            lo[q] = 0.0f;
+                        } else {
+                            hi[q] = acc[0][j][c0 + q][row];
+                            lo[q] = acc[1][j][c0 + q][row];
+                            df_add(hi[q], lo[q], sblk);
+                        }
+                    }
+                    if (!last) {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            acc[0][j][c0 + q][row] = hi[q];
+                            acc[1][j][c0 + q][row] = lo[q];
+                        }
+                    } else {
+                        const int t = j ? t1 : t0;
+                        if (t < p.T) {
+#pragma unroll
+                            for (int jb = 0; jb < 2; ++jb) {
+                                const int bm = c0 / 4 + jb;
+                                if (bm >= b_cnt) continue;
+                                double v[4];
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) v[q] = (double)hi[4 * jb + q] + (double)lo[4 * jb + q];
+                                tc_store_F<SPIN>(p, F_all, b_lo + bm, SPIN ? j : 0, t, m, lmin, v);
+                            }
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sm.accEmpty);
+                ++bk;
+            }
+        }
+        if (ok && nck == 0) {
+            // no representable term in this tile: the rows are exactly zero
+            const int b_lo = (it / nitems) * BM, b_cnt = min(BM, nb - b_lo);
+            const double z[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int t = j ? t1 : t0;
+                if (t < p.T)
+                    for (int bm = 0; bm < b_cnt; ++bm) tc_store_F<SPIN>(p, F_all, b_lo + bm, SPIN ? j : 0, t, m, lmin, z);
+            }
+        }
+        id = id_next;
+        id_next = id_nn;
+        lmin = lmin_n;
+        lwv = lw_n;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            st[j] = st_n[j];
+            stsc[j] = stsc_n[j];
+        }
+    }
+    if (!ok) tc_fail(&sm.fail, p.err);
+}
+
+// ---------------------------------------------------------------------------------
+// builder warps: B tiles (c_l a_lm with the N/S sign pattern) and coefficients
+// ---------------------------------------------------------------------------------
+struct TcLoad {
+    double c;
+    double2 e, b, ag;
+    bool live;  // a chunk exists (values past the column or the batch are zero)
+};
+
+// Walks the CTA's (item, chunk) sequence, skipping items without chunks.
+template <int BM>
+struct TcCursor {
+    int it, c, total, nitems, nb;
+    TcItem q;
+    __device__ __forceinline__ void settle(const TcParams &p) {
+        while (it < total) {
+            q = tc_item(p, it, nitems, nb, BM);
+            if (q.nck > 0) return;
+            it += gridDim.x;
+        }
+    }
+    __device__ __forceinline__ void next(const TcParams &p) {
+        if (it >= total) return;
+        if (++c >= q.nck) {
+            c = 0;
+            it += gridDim.x;
+            settle(p);
+        }
+    }
+};
+
+template <int SPIN, int BM>
+__device__ __forceinline__ TcLoad tc_load(const TcParams &p, const double2 *__restrict__ alm_all,
+                                          const TcCursor<BM> &cur, int k, int bm) {
+    TcLoad r;
+    r.c = 0.0;
+    r.e = r.b = r.ag = make_double2(0.0, 0.0);
+    r.live = cur.it < cur.total;
+    if (!r.live) return r;
+    const int i = cur.q.i_start + cur.c * kTcK + k;
+    if (i >= cur.q.nst) return r;
+    const long long idx = cur.q.b0 + i;
+    if (bm == 0) r.ag = make_double2(__ldg(&p.alpha[idx]), SPIN ? __ldg(&p.gamma[idx]) : 0.0);
+    if (bm >= cur.q.b_cnt) return r;
+    r.c = __ldg(&p.cnorm[idx]);
+    if (SPIN) {
+        r.e = __ldg(&alm_all[((size_t)(cur.q.b_lo + bm) * 2) * p.K + idx]);
+        r.b = __ldg(&alm_all[((size_t)(cur.q.b_lo + bm) * 2 + 1) * p.K + idx]);
+    } else {
+        r.e = __ldg(&alm_all[(size_t)(cur.q.b_lo + bm) * p.K + idx]);
+    }
+    return r;
+}
+
+template <int SPIN, int BM>
+__device__ void tc_builder(const TcParams &p, const double2 *__restrict__ alm_all, TcSmem<SPIN, BM> &sm, int nb,
+                           int bt, int lane) {
+    using C = TcCfg<SPIN, BM>;
+    const int k = bt % kTcK, bm = bt / kTcK;
+    const double sg = (k & 1) ? -1.0 : 1.0;  // (-1)^(l - lmin): chunks start at even offsets
+    const int nitems = p.M * p.ntiles;
+    // the loads run two chunks ahead of the stores
+    TcCursor<BM> ld{(int)blockIdx.x, 0, nitems * ((nb + BM - 1) / BM), nitems, nb, TcItem{}};
+    ld.settle(p);
+    TcLoad r0 = tc_load<SPIN, BM>(p, alm_all, ld, k, bm);
+    ld.next(p);
+    TcLoad r1 = tc_load<SPIN, BM>(p, alm_all, ld, k, bm);
+    ld.next(p);
+    unsigned gc = 0;
+    bool ok = true;
+    while (r0.live) {
+        if (tc_failed(&sm.fail)) break;
+        const int sB = gc % C::NSB;
+        if (gc >= (unsigned)C::NSB && !mbar_wait(&sm.emptyB[sB], ((gc / C::NSB) - 1u) & 1u)) { ok = false; break; }
+        double col[C::NBT][4];
+        if (SPIN) {
+            // cp = -(aE + i aB) c, cm = -(aE - i aB) c   (healpix.py:316-318)
+            const double cpr = -(r0.e.x - r0.b.y) * r0.c, cpi = -(r0.e.y + r0.b.x) * r0.c;
+            const double cmr = -(r0.e.x + r0.b.y) * r0.c, cmi = -(r0.e.y - r0.b.x) * r0.c;
+            col[0][0] = cpr; col[0][1] = cpi; col[0][2] = sg * cmr; col[0][3] = sg * cmi;
+            col[C::NBT - 1][0] = cmr; col[C::NBT - 1][1] = cmi; col[C::NBT - 1][2] = sg * cpr; col[C::NBT - 1][3] = sg * cpi;
+        } else {
+            col[0][0] = r0.e.x * r0.c; col[0][1] = r0.e.y * r0.c;
+            col[0][2] = sg * r0.e.x * r0.c; col[0][3] = sg * r0.e.y * r0.c;
+        }
+#pragma unroll
+        for (int hh = 0; hh < C::NBT; ++hh)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                __nv_bfloat16 vh, vm, vl;
+                split3(col[hh][j], vh, vm, vl);
+                const uint32_t off = kmaj_off(4 * bm + j, k);
+                *reinterpret_cast<__nv_bfloat16 *>(sm.B[sB][hh][0] + off) = vh;
+                *reinterpret_cast<__nv_bfloat16 *>(sm.B[sB][hh][1] + off) = vm;
+                *reinterpret_cast<__nv_bfloat16 *>(sm.B[sB][hh][2] + off) = vl;
+            }
+        if (bm == 0) sm.coef[sB][k] = r0.ag;
+        fence_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.fullB[sB]);
+        ++gc;
+        r0 = r1;
+        r1 = tc_load<SPIN, BM>(p, alm_all, ld, k, bm);
+        ld.next(p);
+    }
+    if (!ok) tc_fail(&sm.fail, p.err);
+}
+
+// ---------------------------------------------------------------------------------
+// MMA warp: one thread issues the split products and the commits
+// ---------------------------------------------------------------------------------
+template <int SPIN, int BM>
+__device__ void tc_mma(const TcParams &p, TcSmem<SPIN, BM> &sm, int nb, uint32_t tbase, int lane) {
+    using C = TcCfg<SPIN, BM>;
+    constexpr int N = C::N;
     constexpr uint32_t IDESC = idesc_bf16(kTcRows, N);
+    const int nitems = p.M * p.ntiles;
+    const int total = nitems * ((nb + BM - 1) / BM);
+    unsigned gc = 0, bk = 0;
+    bool ok = true;
+    const int stride = gridDim.x;
+    int it = blockIdx.x;
+    int id_next = tc_order(p, it + stride, nitems, total);
+    int nck_cur = it < total ? tc_item(p, it, nitems, nb, BM).nck : 0;
+    for (; it < total && ok; it += stride) {
+        if (tc_failed(&sm.fail)) break;
+        const int id_nn = tc_order(p, it + 2 * stride, nitems, total);
+        const int nck_next = tc_item_of(p, it + stride < total ? it + stride : it, id_next, nitems, nb, BM).nck;
+        const int nck = nck_cur;
+        for (int c = 0; c < nck; ++c, ++gc) {
+            const int sA = gc % C::NSA, sB = gc % C::NSB;
+            const bool bstart = (c % kFlush) == 0;
+            const bool bend = (c % kFlush) == kFlush - 1 || c == nck - 1;
+            if (!mbar_wait(&sm.fullA[sA], (gc / C::NSA) & 1u) || !mbar_wait(&sm.fullB[sB], (gc / C::NSB) & 1u) ||
+                (bstart && bk > 0 && !mbar_wait(&sm.accEmpty, (bk - 1u) & 1u))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            if (lane == 0) {
+                const uint32_t acc = bstart ? 0u : 1u;
+#pragma unroll
+                for (int j = 0; j < C::NG; ++j) {
+                    const int jb = SPIN ? j : 0;
+                    const uint32_t d = tbase + (uint32_t)(j * 2 * N), dc = d + (uint32_t)N;
+                    const uint32_t a0 = tbase + (uint32_t)(C::COL_A + (sA * C::NG + j) * 3 * C::ACOLS);
+                    const uint32_t a1 = a0 + C::ACOLS, a2 = a0 + 2 * C::ACOLS;
+                    const uint64_t c0 = smem_desc(sm.B[sB][jb][0], 128, 256), c1 = smem_desc(sm.B[sB][jb][1], 128, 256),
+                                   c2 = smem_desc(sm.B[sB][jb][2], 128, 256);
+                    umma_f16_ts(d, a0, c0, IDESC, acc);   // hh
+                    umma_f16_ts(dc, a0, c1, IDESC, acc);  // hm
+                    umma_f16_ts(dc, a1, c0, IDESC, 1u);   // mh
+                    umma_f16_ts(dc, a0, c2, IDESC, 1u);   // hl
+                    umma_f16_ts(dc, a2, c0, IDESC, 1u);   // lh
+                    umma_f16_ts(dc, a1, c1, IDESC, 1u);   // mm
+                }
+                umma_commit(&sm.emptyA[sA]);
+                umma_commit(&sm.emptyB[sB]);
+                if (bend) umma_commit(&sm.accFull);
+            }
+            __syncwarp();
+            if (bend) ++bk;
+        }
+        nck_cur = nck_next;
+        id_next = id_nn;
+    }
+    if (!ok) tc_fail(&sm.fail, p.err);
+    // every issued MMA has completed before tensor memory is released
+    if (lane == 0) {
+        umma_commit(&sm.fin);
+        if (!mbar_wait(&sm.fin, 0u)) tc_fail(&sm.fail, p.err);
+    }
+    __syncwarp();
+}
+
+template <int SPIN, int BM>
+__global__ void __launch_bounds__(TcCfg<SPIN, BM>::NTHREADS, 2)
+    tc_synth_kernel(TcParams p, const double2 *__restrict__ alm_all, double2 *__restrict__ F_all, int nb) {
+    using C = TcCfg<SPIN, BM>;
+    using S = TcSmem<SPIN, BM>;
     extern __shared__ unsigned char smem_raw[];
     S &sm = *reinterpret_cast<S *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    __shared__ int s_it;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int row = tid % kTcRows;  // ring within the tile = A row = TMEM lane
-    const int h = tid / kTcRows;    // recursion: 0 = +spin (or spin 0), 1 = -spin
-    const double gsign = h ? -1.0 : 1.0;
-
-    if (warp == 0) {
-        tmem_alloc(&sm.taddr, TCOLS);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == C::MMA_WARP) {
+        tmem_alloc(&sm.taddr, C::TCOLS);
         tmem_relinquish();
     }
-    if (tid == 0) {
-        mbar_init(&sm.mbar[0], 1);
-        mbar_init(&sm.mbar[1], 1);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < C::NSA; ++s) {
+            mbar_init(&sm.fullA[s], C::NPW);
+            mbar_init(&sm.emptyA[s], 1);
+        }
+        for (int s = 0; s < C::NSB; ++s) {
+            mbar_init(&sm.fullB[s], C::NBW);
+            mbar_init(&sm.emptyB[s], 1 + C::NPW);
+        }
+        mbar_init(&sm.accFull, 1);
+        mbar_init(&sm.accEmpty, C::NPW);
+        mbar_init(&sm.fin, 1);
+        sm.fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tbase = sm.taddr;
-    const uint32_t tlane = (uint32_t)((warp & 3) * 32) << 16;
-    uint32_t phase[2] = {0u, 0u};
-    bool pending[2] = {false, false};
-    bool failed = false;
-
-    const int L = p.lmax;
-    const int ngroups = (nb + BM - 1) / BM;
-    const int nitems = p.M * p.ntiles;
-    for (;;) {
-        if (tid == 0) s_it = (int)atomicAdd(p.counter, 1u);
-        __syncthreads();
-        const int it = s_it;
-        __syncthreads();
-        if (it >= nitems * ngroups || failed) break;
-        const int g = it / nitems;
-        const int item = p.order[it - g * nitems];
-        const int m = item / p.ntiles, tile = item % p.ntiles;
-        const int b_lo = g * BM, b_cnt = min(BM, nb - b_lo);
-        const SeedParam sd = p.seed[m];
-        const long long b0 = alm_index(sd.lmin, m, L);
-        const int nst = L - sd.lmin + 1;
-        const int i_start = p.lw[item] - sd.lmin;
-        const int t = tile * kTcRows + row;
-        const bool valid = t < p.T;
-        const double x = valid ? p.x[t] : 0.0;
-        double u1, u2;
-        int sc;
-        {
-            // start-state layout [item][h][r][lane], ring = r * 32 + lane within the tile
-            const size_t o = ((size_t)item * NG + h) * kTcRows + row;
-            const double2 st = p.st[o];
-            u1 = st.x;
-            u2 = st.y;
-            sc = valid ? p.stsc[o] : 0;
-        }
-        bool fast = sc == 0;
-        double acc[N];
-#pragma unroll
-        for (int n = 0; n < N; ++n) acc[n] = 0.0;
-        bool fresh = true;
-        int kc = 0;
-        for (int i0 = i_start; i0 < nst; i0 += kTcK, ++kc) {
-            const int s = kc & 1;
-            if (pending[s]) {
-                if (!mbar_wait(&sm.mbar[s], phase[s])) failed = true;
-                phase[s] ^= 1u;
-                pending[s] = false;
-            }
-            if (kc % kSuper == 0) {
-                // ---- staging pass for kSuper chunks; the pipeline is drained here (the
-                //      previous chunk closed a flush block). ----
-                for (int w = tid; w < kSuper * kTcK; w += NTH) {
-                    const int i = i0 + w;
-                    sm.coef[w] = i < nst ? make_double2(p.alpha[b0 + i], SPIN ? p.gamma[b0 + i] : 0.0)
-                                         : make_double2(0.0, 0.0);
-                }
-                for (int w = tid; w < kSuper * kTcK * BM; w += NTH) {
-                    const int st = w % (kSuper * kTcK), bm = w / (kSuper * kTcK);
-                    const int k = st % kTcK, cix = st / kTcK;
-                    const int i = i0 + st;
-                    const double sg = (k & 1) ? -1.0 : 1.0;  // (-1)^(l - lmin): chunks start at even i
-                    double col[NG][4];
-                    if (i < nst && bm < b_cnt) {
-                        const long long idx = b0 + i;
-                        const double c = p.cnorm[idx];
-                        if (SPIN) {
-                            const double2 e = alm_all[((size_t)(b_lo + bm) * 2) * p.K + idx];
-                            const double2 bb = alm_all[((size_t)(b_lo + bm) * 2 + 1) * p.K + idx];
-                            // cp = -(aE + i aB) c, cm = -(aE - i aB) c   (healpix.py:316-318)
-                            const double cpr = -(e.x - bb.y) * c, cpi = -(e.y + bb.x) * c;
-                            const double cmr = -(e.x + bb.y) * c, cmi = -(e.y - bb.x) * c;
-                            col[0][0] = cpr; col[0][1] = cpi; col[0][2] = sg * cmr; col[0][3] = sg * cmi;
-                            col[NG - 1][0] = cmr; col[NG - 1][1] = cmi; col[NG - 1][2] = sg * cpr; col[NG - 1][3] = sg * cpi;
-                        } else {
-                            const double2 a = alm_all[(size_t)(b_lo + bm) * p.K + idx];
-                            col[0][0] = a.x * c; col[0][1] = a.y * c; col[0][2] = sg * a.x * c; col[0][3] = sg * a.y * c;
-                        }
-                    } else {
-#pragma unroll
-                        for (int hh = 0; hh < NG; ++hh)
-#pragma unroll
-                            for (int j = 0; j < 4; ++j) col[hh][j] = 0.0;
-                    }
-#pragma unroll
-                    for (int hh = 0; hh < NG; ++hh)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            __nv_bfloat16 vh, vm, vl;
-                            split3(col[hh][j], vh, vm, vl);
-                            const uint32_t off = kmaj_off(4 * bm + j, k);
-                            *reinterpret_cast<__nv_bfloat16 *>(sm.B[cix][hh][0] + off) = vh;
-                            *reinterpret_cast<__nv_bfloat16 *>(sm.B[cix][hh][1] + off) = vm;
-                            *reinterpret_cast<__nv_bfloat16 *>(sm.B[cix][hh][2] + off) = vl;
-                        }
-                }
-            }
-            if (__syncthreads_or(failed)) {
-                failed = true;
-                break;
-            }
-            // ---- A: 16 steps of this thread's recursion, split into BF16 parts ----
-            const int ncnt = min(kTcK, nst - i0);
-            const double2 *coef = sm.coef + (kc % kSuper) * kTcK;
-            uint32_t pk[3][kTcK / 2];
-            if (__all_sync(0xffffffffu, fast)) {
-                tc_chunk<false>(coef, ncnt, x, gsign, valid, u1, u2, sc, pk);
-            } else {
-                tc_chunk<true>(coef, ncnt, x, gsign, valid, u1, u2, sc, pk);
-                fast = sc == 0;
-            }
-#pragma unroll
-            for (int sp = 0; sp < 3; ++sp) {
-                unsigned char *Ab = sm.A[s][h][sp];
-                *reinterpret_cast<uint4 *>(Ab + kmaj_off(row, 0)) = make_uint4(pk[sp][0], pk[sp][1], pk[sp][2], pk[sp][3]);
-                *reinterpret_cast<uint4 *>(Ab + kmaj_off(row, 8)) = make_uint4(pk[sp][4], pk[sp][5], pk[sp][6], pk[sp][7]);
-            }
-            fence_async_smem();
-            __syncthreads();
-            // ---- one thread issues the split products; a commit frees stage s ----
-            if (tid == 0) {
-                tc_fence_after();
-                const int bs = kc % kSuper;
-#pragma unroll
-                for (int hh = 0; hh < NG; ++hh) {
-                    // hh into its own accumulator; the five smaller products (relative size
-                    // <= 2^-8) into a second one, so hh sees 4 FP32 roundings per block
-                    const uint32_t d = tbase + (uint32_t)(hh * 2 * N), dc = d + (uint32_t)N;
-                    const uint64_t a0 = smem_desc(sm.A[s][hh][0], 128, 256), a1 = smem_desc(sm.A[s][hh][1], 128, 256),
-                                   a2 = smem_desc(sm.A[s][hh][2], 128, 256);
-                    const uint64_t c0 = smem_desc(sm.B[bs][hh][0], 128, 256), c1 = smem_desc(sm.B[bs][hh][1], 128, 256),
-                                   c2 = smem_desc(sm.B[bs][hh][2], 128, 256);
-                    umma_f16(d, a0, c0, IDESC, fresh ? 0u : 1u);   // hh
-                    umma_f16(dc, a0, c1, IDESC, fresh ? 0u : 1u);  // hm
-                    umma_f16(dc, a1, c0, IDESC, 1u);               // mh
-                    umma_f16(dc, a0, c2, IDESC, 1u);               // hl
-                    umma_f16(dc, a2, c0, IDESC, 1u);               // lh
-                    umma_f16(dc, a1, c1, IDESC, 1u);               // mm
-                }
-                umma_commit(&sm.mbar[s]);
-            }
-            pending[s] = true;
-            fresh = false;
-            const bool last = i0 + kTcK >= nst;
-            if ((kc % kFlush) == kFlush - 1 || last) {
-                // drain both stages (older first), then fold the FP32 block into FP64
-                const int so = s ^ 1;
-                if (pending[so]) {
-                    if (!mbar_wait(&sm.mbar[so], phase[so])) failed = true;
-                    phase[so] ^= 1u;
-                    pending[so] = false;
-                }
-                if (!mbar_wait(&sm.mbar[s], phase[s])) failed = true;
-                phase[s] ^= 1u;
-                pending[s] = false;
-                tc_fence_after();
-                if (__syncthreads_or(failed)) {
-                    failed = true;
-                    break;
-                }
-#pragma unroll
-                for (int part = 0; part < 2; ++part)
-#pragma unroll
-                    for (int c0 = 0; c0 < N; c0 += 32) {
-                        float v[32];
-                        tmem_ld32(tbase + tlane + (uint32_t)(h * 2 * N + part * N + c0), v);
-#pragma unroll
-                        for (int j = 0; j < 32; ++j)
-                            if (c0 + j < N) acc[c0 + j] += (double)v[j];
-                    }
-                tc_fence_before();
-                __syncthreads();
-                fresh = true;
-            }
-        }
-        if (failed) break;
-        // ---- outputs: F_north / F_south per map (healpix.py:250-253) ----
-        if (valid) {
-            const double ssign = ((m + sd.lmin) & 1) ? -1.0 : 1.0;
-            const size_t rs = (size_t)(4 * p.nside - 2 - t);
-            for (int bm = 0; bm < b_cnt; ++bm) {
-                if (SPIN) {
-                    // GEMM + (h = 0): [FpN | FmS signed];  GEMM - (h = 1): [FmN | FpS signed]
-                    double2 *Fp = F_all + (size_t)(b_lo + bm) * 2 * p.nrings * p.M;
-                    double2 *Fm = Fp + (size_t)p.nrings * p.M;
-                    double2 *Fn = h ? Fm : Fp, *Fs = h ? Fp : Fm;
-                    Fn[(size_t)t * p.M + m] = make_double2(acc[4 * bm], acc[4 * bm + 1]);
-                    if (t < p.T - 1) Fs[rs * p.M + m] = make_double2(ssign * acc[4 * bm + 2], ssign * acc[4 * bm + 3]);
-                } else {
-                    double2 *F = F_all + (size_t)(b_lo + bm) * p.nrings * p.M;
-                    F[(size_t)t * p.M + m] = make_double2(acc[4 * bm], acc[4 * bm + 1]);
-                    if (t < p.T - 1) F[rs * p.M + m] = make_double2(acc[4 * bm + 2], acc[4 * bm + 3]);
-                }
-            }
-        }
+    if (warp < C::NPW) {
+        tc_producer<SPIN, BM>(p, sm, F_all, nb, tbase, warp, lane);
+    } else if (warp < C::NPW + C::NBW) {
+        tc_builder<SPIN, BM>(p, alm_all, sm, nb, threadIdx.x - C::NPW * 32, lane);
+    } else {
+        tc_mma<SPIN, BM>(p, sm, nb, tbase, lane);
     }
-    if (failed && tid == 0) atomicExch(p.err, 1);
-    // release tensor memory once every issued MMA has completed (bounded)
-    for (int s = 0; s < 2; ++s)
-        if (pending[s]) {
-            mbar_wait(&sm.mbar[s], phase[s]);
-            pending[s] = false;
-        }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 0) tmem_dealloc(tbase, TCOLS);
+    if (warp == C::MMA_WARP) tmem_dealloc(tbase, C::TCOLS);
 }
 
 }  // namespace
@@ -469,9 +740,33 @@ int tc_smem_bytes(int spin) {
     return (spin ? (int)sizeof(TcSmem<2, kTcMaps>) : (int)sizeof(TcSmem<0, kTcMaps>)) + 1024;
 }
 
+template <int SPIN>
+static int launch_tc_synth_t(const TcParams &q, const double2 *alm, double2 *F, int nb, cudaStream_t s) {
+    using C = TcCfg<SPIN, kTcMaps>;
+    auto k = tc_synth_kernel<SPIN, kTcMaps>;
+    const int smem = tc_smem_bytes(SPIN);
+    int dev = 0, nsm = 148, smem_sm = 0, regs_sm = 0, resv = 0;
+    JHTB_CUDA_TRY(cudaGetDevice(&dev));
+    JHTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    JHTB_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    JHTB_CUDA_TRY(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    JHTB_CUDA_TRY(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    JHTB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    JHTB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    cudaFuncAttributes fa;
+    JHTB_CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+    // resident CTAs per SM by shared memory, registers and tensor memory (512 columns:
+    // a resident CTA must never wait on tensor memory held by another)
+    int per_sm = smem_sm / (smem + resv);
+    per_sm = std::min(per_sm, regs_sm / std::max(1, fa.numRegs * C::NTHREADS));
+    per_sm = std::max(1, std::min(per_sm, (int)(512 / C::TCOLS)));
+    k<<<nsm * per_sm, C::NTHREADS, smem, s>>>(q, alm, F, nb);
+    JHTB_CUDA_TRY(cudaGetLastError());
+    return JHTB_OK;
+}
+
 int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;
-    JHTB_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned), s));
     TcParams q;
     q.lmax = p.lmax;
     q.T = p.T;
@@ -489,25 +784,8 @@ int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaS
     q.st = p.d_tc_st;
     q.stsc = p.d_tc_stsc;
     q.order = p.d_tc_order;
-    q.counter = p.d_counter;
     q.err = p.d_err;
-    const int smem = tc_smem_bytes(p.spin);
-    int dev = 0, nsm = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (p.spin) {
-        auto k = tc_synth_kernel<2, kTcMaps>;
-        JHTB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 2 * kTcRows, smem);
-        k<<<nsm * std::max(2, per_sm), 2 * kTcRows, smem, s>>>(q, alm, F, nb);
-    } else {
-        auto k = tc_synth_kernel<0, kTcMaps>;
-        JHTB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTcRows, smem);
-        k<<<nsm * std::max(2, per_sm), kTcRows, smem, s>>>(q, alm, F, nb);
-    }
-    JHTB_CUDA_TRY(cudaGetLastError());
-    return JHTB_OK;
+    return p.spin ? launch_tc_synth_t<2>(q, alm, F, nb, s) : launch_tc_synth_t<0>(q, alm, F, nb, s);
 }
 
 }  // namespace jhtb
