@@ -7,7 +7,9 @@
 //   adjoint    W[k] = sum_j v[j] e^{-2 pi i jk/N};  V[m] = W[m mod N] e^{-i m phi0}
 //              (spin 2 also Vm[m] = conj(W[-m mod N]) e^{-i m phi0})
 // The fold is a gather (each k collects its own m's), never a scatter.  Power-of-two
-// rings up to 8192 use a radix-2 FFT in shared memory; every other length uses
+// rings up to 8192 use an in-place Stockham FFT in shared memory (radix-16 passes held
+// in registers, natural order in and out, a padded layout against bank conflicts);
+// every other length uses
 // Bluestein's chirp-z with an exact (n^2 mod 2N) chirp argument (_azimuth.py:150-191)
 // at a power-of-two length P >= 2N-1, split into Q = P/8192 shared-memory pieces when
 // P > 8192 (decimation in frequency on the input, twiddled recombination on the output).
@@ -28,7 +30,22 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double2 conjd(double2 a) { return make_double2(a.x, -a.y); }
 
 __device__ __forceinline__ int ilog2i(int n) { return 31 - __clz(n); }
-__device__ __forceinline__ int brev(int k, int logn) { return logn ? (int)(__brev((unsigned)k) >> (32 - logn)) : 0; }
+
+// e^{i pi (a / N + 2 c / P)} for integers a, c and P a power of two: a is reduced
+// exactly modulo 2N and c modulo P before the one rounding of the argument.  Every
+// phase of the azimuthal stage is of this form: on the HEALPix grid phi0 is 0 or
+// pi / N (healpix.py:107-140), so e^{i m phi0} = e^{i pi m / N}; the chirp-z factors are
+// e^{+-i pi n^2 / N} (_azimuth.py:150-191) and the split-length twiddles e^{+-2 pi i s k / P}.
+__device__ __forceinline__ double2 cis_pi(int a, int N, int c, int P) {
+    const int n2 = 2 * N;
+    int r = a % n2;
+    if (r < 0) r += n2;
+    int q = c % P;
+    if (q < 0) q += P;
+    double s, co;
+    sincospi((double)r / (double)N + 2.0 * (double)q / (double)P, &s, &co);
+    return make_double2(co, s);
+}
 
 // e^{i * sgn * pi * (n^2 mod 2N) / N}: the exact chirp-z argument reduction.
 __device__ __forceinline__ double2 chirp(long long n, int N, double sgn) {
@@ -46,46 +63,130 @@ __device__ __forceinline__ double2 root(long long a, long long b, double sgn) {
     return make_double2(c, s);
 }
 
-// In-place radix-2 DIT FFT of length n (power of two <= kFftMax) on shared memory.
-// Input in bit-reversed order, output natural.  dir = -1: e^{-2 pi i jk/n}; +1: e^{+...}.
-__device__ void fft_smem(double2 *buf, int n, int dir, const double2 *__restrict__ tw) {
-    const int logn = ilog2i(n);
-    for (int s = 1; s <= logn; ++s) {
-        const int half = 1 << (s - 1);
-        const int shift = kFftLogMax - s;
-        for (int bf = threadIdx.x; bf < (n >> 1); bf += blockDim.x) {
-            const int k = bf & (half - 1);
-            const int i0 = ((bf >> (s - 1)) << s) + k;
-            const int i1 = i0 + half;
-            double2 w = __ldg(&tw[k << shift]);
-            if (dir > 0) w.y = -w.y;
-            const double2 a = buf[i0];
-            const double2 t = cmul(buf[i1], w);
-            buf[i0] = cadd(a, t);
-            buf[i1] = csub(a, t);
-        }
-        __syncthreads();
+// Shared-memory layout of an FFT buffer: one pad slot every 16 and every 256 elements,
+// so the strided accesses of the Stockham passes spread over the banks.
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4) + (i >> 8); }
+constexpr int kFftBufLen = kFftMax + kFftMax / 16 + kFftMax / 256;
+
+// cos and sin of k pi / 8, k < 8 (the 16th roots of unity)
+__host__ __device__ constexpr double cos16(int k) {
+    return k == 0 ? 1.0 : k == 1 ? 0.9238795325112867 : k == 2 ? 0.7071067811865476 : k == 3 ? 0.3826834323650898
+         : k == 4 ? 0.0 : k == 5 ? -0.3826834323650898 : k == 6 ? -0.7071067811865476 : -0.9238795325112867;
+}
+__host__ __device__ constexpr double sin16(int k) { return cos16(k <= 4 ? 4 - k : k - 4); }
+__host__ __device__ constexpr int brev_ct(int i, int bits) {
+    int r = 0;
+    for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
+    return r;
+}
+__host__ __device__ constexpr int ilog2_ct(int n) { return n <= 1 ? 0 : 1 + ilog2_ct(n / 2); }
+
+// R-point DFT in registers (R <= 16), natural order in and out: radix-2 DIT after a
+// bit-reversal permutation, all indices and roots fixed at compile time.
+// dir = -1: e^{-2 pi i jk/R}; +1: e^{+...}.
+template <int R, int LEN, int I, int K>
+__device__ __forceinline__ void rf_bfly(double2 (&v)[R], double dir) {
+    constexpr int h = LEN / 2, ROOT = K * (16 / LEN);  // e^{dir 2 pi i ROOT / 16}
+    const double2 a = v[I + K];
+    double2 b = v[I + K + h];
+    if constexpr (ROOT == 4) b = make_double2(-dir * b.y, dir * b.x);
+    else if constexpr (ROOT != 0) b = cmul(b, make_double2(cos16(ROOT), dir * sin16(ROOT)));
+    v[I + K] = cadd(a, b);
+    v[I + K + h] = csub(a, b);
+}
+template <int R, int LEN, int IDX>
+__device__ __forceinline__ void rf_stage(double2 (&v)[R], double dir) {
+    if constexpr (IDX < R / 2) {
+        constexpr int h = LEN / 2;
+        rf_bfly<R, LEN, (IDX / h) * LEN, IDX % h>(v, dir);
+        rf_stage<R, LEN, IDX + 1>(v, dir);
     }
 }
-
-// In-place radix-2 DIF FFT: input natural order, output bit-reversed.
-__device__ void fft_smem_dif(double2 *buf, int n, int dir, const double2 *__restrict__ tw) {
-    const int logn = ilog2i(n);
-    for (int s = logn; s >= 1; --s) {
-        const int half = 1 << (s - 1);
-        const int shift = kFftLogMax - s;
-        for (int bf = threadIdx.x; bf < (n >> 1); bf += blockDim.x) {
-            const int k = bf & (half - 1);
-            const int i0 = ((bf >> (s - 1)) << s) + k;
-            const int i1 = i0 + half;
-            double2 w = __ldg(&tw[k << shift]);
-            if (dir > 0) w.y = -w.y;
-            const double2 a = buf[i0], b = buf[i1];
-            buf[i0] = cadd(a, b);
-            buf[i1] = cmul(csub(a, b), w);
-        }
-        __syncthreads();
+template <int R, int LEN>
+__device__ __forceinline__ void rf_stages(double2 (&v)[R], double dir) {
+    if constexpr (LEN <= R) {
+        rf_stage<R, LEN, 0>(v, dir);
+        rf_stages<R, LEN * 2>(v, dir);
     }
+}
+template <int R, int I>
+__device__ __forceinline__ void rf_bitrev(double2 (&v)[R]) {
+    if constexpr (I < R) {
+        constexpr int J = brev_ct(I, ilog2_ct(R));
+        if constexpr (J > I) {
+            const double2 t = v[I];
+            v[I] = v[J];
+            v[J] = t;
+        }
+        rf_bitrev<R, I + 1>(v);
+    }
+}
+template <int R>
+__device__ __forceinline__ void reg_fft(double2 (&v)[R], double dir) {
+    rf_bitrev<R, 0>(v);
+    rf_stages<R, 2>(v, dir);
+}
+
+// One in-place Stockham pass of radix R over n points (Ns = product of the earlier
+// radices): every thread loads its R inputs (stride n/R), twiddles them by
+// e^{dir 2 pi i (j mod Ns) r / (Ns R)}, runs an R-point DFT in registers and, after a
+// barrier, stores them at (j / Ns) Ns R + (j mod Ns) + r Ns.  n <= 8192 and 512
+// threads: each thread holds at most 16 points.
+template <int R>
+__device__ __forceinline__ void stockham_pass(double2 *buf, int n, int Ns, double dir,
+                                              const double2 *__restrict__ tw) {
+    constexpr int JM = 16 / R;
+    const int nj = n / R;
+    double2 v[JM][R];
+#pragma unroll
+    for (int jj = 0; jj < JM; ++jj) {
+        const int j = threadIdx.x + jj * kFftThreads;
+        if (j < nj) {
+            const int jm = j & (Ns - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[jj][r] = buf[pidx(j + r * nj)];
+            if (Ns > 1) {
+                const int step = jm * (kFftMax / (Ns * R));
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    double2 w = __ldg(&tw[step * r]);
+                    if (dir > 0) w.y = -w.y;
+                    v[jj][r] = cmul(v[jj][r], w);
+                }
+            }
+            reg_fft<R>(v[jj], dir);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < JM; ++jj) {
+        const int j = threadIdx.x + jj * kFftThreads;
+        if (j < nj) {
+            const int jm = j & (Ns - 1);
+            const int d = (j - jm) * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[pidx(d + r * Ns)] = v[jj][r];
+        }
+    }
+    __syncthreads();
+}
+
+// One pass as a separate function: each radix is compiled once, with its own registers.
+template <int R>
+__device__ __noinline__ void stockham_pass_call(double2 *buf, int n, int Ns, double dir,
+                                                const double2 *__restrict__ tw) {
+    stockham_pass<R>(buf, n, Ns, dir, tw);
+}
+
+// In-place FFT of length n (power of two <= kFftMax) on a padded shared-memory buffer,
+// natural order in and out.  dir = -1: e^{-2 pi i jk/n}; +1: e^{+2 pi i jk/n}.
+// Passes of radix 16 with one smaller radix for the remaining bits.
+__device__ __forceinline__ void fft_stockham(double2 *buf, int n, double dir, const double2 *__restrict__ tw) {
+    int bits = ilog2i(n), Ns = 1;
+    for (; bits >= 4; bits -= 4, Ns <<= 4) stockham_pass_call<16>(buf, n, Ns, dir, tw);
+    if (bits == 3) stockham_pass_call<8>(buf, n, Ns, dir, tw);
+    else if (bits == 2) stockham_pass_call<4>(buf, n, Ns, dir, tw);
+    else if (bits == 1) stockham_pass_call<2>(buf, n, Ns, dir, tw);
 }
 
 // Bluestein spectrum for the synthesis direction: Bh+ = FFT_P(b)/P with
@@ -96,27 +197,34 @@ __device__ __forceinline__ double2 bh_get(const double2 *bh, int P, int k, int s
     return conjd(__ldg(&bh[(P - k) & (P - 1)]));
 }
 
-// D[k] of the synthesis fold for one ring (spin 0 passes Fm == Fp).
+// D[k] of the synthesis fold for one ring, without its phase (spin 0 passes Fm == Fp):
+// with m = k + jN in the first sum and m = jN - k in the second,
+// e^{i m phi0} = (-1)^j e^{+-i pi k / N} when phi0 = pi / N, so
+// D[k] = e^{i pi k / N} [sum_j (-1)^j Fp_{k+jN} + sum_j (-1)^j conj(Fm_{jN-k})];
+// `shifted` selects the (-1)^j signs, the caller applies e^{i pi k / N}.
 __device__ __forceinline__ double2 fold_synth(const double2 *__restrict__ Fp, const double2 *__restrict__ Fm,
-                                              int k, int N, int lmax, double phi0) {
+                                              int k, int N, int lmax, bool shifted) {
     double2 d = make_double2(0.0, 0.0);
+    double sg = 1.0;
     for (int m = k; m <= lmax; m += N) {
-        double s, c;
-        sincos((double)m * phi0, &s, &c);
-        d = cadd(d, cmul(Fp[m], make_double2(c, s)));
+        const double2 f = Fp[m];
+        d.x = fma(sg, f.x, d.x);
+        d.y = fma(sg, f.y, d.y);
+        if (shifted) sg = -sg;
     }
-    int m0 = (N - k) % N;
-    if (m0 == 0) m0 = N;
+    int m0 = N - k;  // m = jN - k, j >= 1
+    sg = shifted ? -1.0 : 1.0;
     for (int m = m0; m <= lmax; m += N) {
-        double s, c;
-        sincos((double)m * phi0, &s, &c);
-        d = cadd(d, conjd(cmul(Fm[m], make_double2(c, s))));
+        const double2 f = Fm[m];
+        d.x = fma(sg, f.x, d.x);
+        d.y = fma(-sg, f.y, d.y);
+        if (shifted) sg = -sg;
     }
     return d;
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads) ring_synth_kernel(const RingDesc *__restrict__ rings, int lmax,
+__global__ void __launch_bounds__(kFftThreads, 1) ring_synth_kernel(const RingDesc *__restrict__ rings, int lmax,
                                                                   int M, int nrings, long long npix,
                                                                   const double2 *__restrict__ F_all,
                                                                   double *__restrict__ maps_all,
@@ -126,44 +234,46 @@ __global__ void __launch_bounds__(kFftThreads) ring_synth_kernel(const RingDesc 
     const int r = blockIdx.x;
     const RingDesc rd = rings[r];
     const int N = rd.N;
+    const bool shifted = rd.phi0 != 0.0;
     constexpr int nchan = SPIN ? 2 : 1;
     const double2 *Fp = F_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     const double2 *Fm = SPIN ? Fp + (size_t)nrings * M : Fp;
     double *outQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     double *outU = outQ + npix;
     if (rd.mode == kDirect) {
-        const int logn = ilog2i(N);
-        for (int k = threadIdx.x; k < N; k += blockDim.x) buf[brev(k, logn)] = fold_synth(Fp, Fm, k, N, lmax, rd.phi0);
+        for (int k = threadIdx.x; k < N; k += blockDim.x) {
+            const double2 d = fold_synth(Fp, Fm, k, N, lmax, shifted);
+            buf[pidx(k)] = shifted ? cmul(d, cis_pi(k, N, 0, 1)) : d;
+        }
         __syncthreads();
-        fft_smem(buf, N, +1, tw);
+        fft_stockham(buf, N, +1.0, tw);
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            outQ[j] = buf[j].x;
-            if (SPIN) outU[j] = buf[j].y;
+            const double2 v = buf[pidx(j)];
+            outQ[j] = v.x;
+            if (SPIN) outU[j] = v.y;
         }
         return;
     }
-    const int P = rd.P, Q = rd.Q, Pp = P / Q, logp = ilog2i(Pp);
+    const int P = rd.P, Q = rd.Q, Pp = P / Q;
     const double2 *B = bh + rd.bh_off;
     for (int s = 0; s < Q; ++s) {
         // piece s of FFT_P(a), a[k] = D[k] w(k): fold a[k] e^{-2 pi i s k / P} modulo Pp
         for (int q = threadIdx.x; q < Pp; q += blockDim.x) {
             double2 v = make_double2(0.0, 0.0);
             for (int k = q; k < N; k += Pp) {
-                double2 a = cmul(fold_synth(Fp, Fm, k, N, lmax, rd.phi0), chirp(k, N, 1.0));
-                if (s) a = cmul(a, root((long long)s * k, P, -1.0));
-                v = cadd(v, a);
+                // D[k] w(k) e^{-2 pi i s k / P}, w(k) = e^{i pi k^2 / N}, with the ring phase folded in
+                const int ph = (k * k) % (2 * N) + (shifted ? k : 0);
+                v = cadd(v, cmul(fold_synth(Fp, Fm, k, N, lmax, shifted), cis_pi(ph, N, -s * k, P)));
             }
-            buf[brev(q, logp)] = v;
+            buf[pidx(q)] = v;
         }
         __syncthreads();
-        fft_smem(buf, Pp, -1, tw);
-        for (int q = threadIdx.x; q < Pp; q += blockDim.x) buf[q] = cmul(buf[q], bh_get(B, P, Q * q + s, 1));
+        fft_stockham(buf, Pp, -1.0, tw);
+        for (int q = threadIdx.x; q < Pp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, P, Q * q + s, 1));
         __syncthreads();
-        fft_smem_dif(buf, Pp, +1, tw);  // output in bit-reversed order
+        fft_stockham(buf, Pp, +1.0, tw);
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            double2 v = buf[brev(j & (Pp - 1), logp)];
-            if (s) v = cmul(v, root((long long)s * j, P, 1.0));
-            v = cmul(v, chirp(j, N, 1.0));
+            const double2 v = cmul(buf[pidx(j & (Pp - 1))], cis_pi((j * j) % (2 * N), N, s * j, P));
             if (s == 0) {
                 outQ[j] = v.x;
                 if (SPIN) outU[j] = v.y;
@@ -176,21 +286,26 @@ __global__ void __launch_bounds__(kFftThreads) ring_synth_kernel(const RingDesc 
     }
 }
 
-// V rows for ring r from its spectrum W (smem or global).
-template <int SPIN>
-__device__ __forceinline__ void gather_adjoint(const double2 *W, int N, int lmax, double phi0, double2 *Vp,
+// V rows for ring r from its spectrum W (padded shared-memory buffer or natural global).
+template <int SPIN, bool PADDED>
+__device__ __forceinline__ void gather_adjoint(const double2 *W, int N, int lmax, bool shifted, double2 *Vp,
                                                double2 *Vm) {
     for (int m = threadIdx.x; m <= lmax; m += blockDim.x) {
-        double s, c;
-        sincos((double)m * phi0, &s, &c);
-        const double2 cph = make_double2(c, -s);
-        Vp[m] = cmul(W[m % N], cph);
-        if (SPIN) Vm[m] = cmul(conjd(W[(N - m % N) % N]), cph);
+        const int k1 = m % N, k2 = (N - k1) % N;
+        double2 vp = W[PADDED ? pidx(k1) : k1];
+        double2 vm = SPIN ? conjd(W[PADDED ? pidx(k2) : k2]) : vp;
+        if (shifted) {  // e^{-i m phi0} = e^{-i pi m / N}
+            const double2 cph = cis_pi(-(m % (2 * N)), N, 0, 1);
+            vp = cmul(vp, cph);
+            vm = cmul(vm, cph);
+        }
+        Vp[m] = vp;
+        if (SPIN) Vm[m] = vm;
     }
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads) ring_adjoint_kernel(const RingDesc *__restrict__ rings, int lmax,
+__global__ void __launch_bounds__(kFftThreads, 1) ring_adjoint_kernel(const RingDesc *__restrict__ rings, int lmax,
                                                                     int M, int nrings, long long npix,
                                                                     const double *__restrict__ maps_all,
                                                                     double2 *__restrict__ V_all,
@@ -201,49 +316,43 @@ __global__ void __launch_bounds__(kFftThreads) ring_adjoint_kernel(const RingDes
     const int r = blockIdx.x;
     const RingDesc rd = rings[r];
     const int N = rd.N;
+    const bool shifted = rd.phi0 != 0.0;
     constexpr int nchan = SPIN ? 2 : 1;
     const double *inQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     const double *inU = inQ + npix;
     double2 *Vp = V_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     double2 *Vm = SPIN ? Vp + (size_t)nrings * M : Vp;
     if (rd.mode == kDirect) {
-        const int logn = ilog2i(N);
-        for (int j = threadIdx.x; j < N; j += blockDim.x)
-            buf[brev(j, logn)] = make_double2(inQ[j], SPIN ? inU[j] : 0.0);
+        for (int j = threadIdx.x; j < N; j += blockDim.x) buf[pidx(j)] = make_double2(inQ[j], SPIN ? inU[j] : 0.0);
         __syncthreads();
-        fft_smem(buf, N, -1, tw);
-        gather_adjoint<SPIN>(buf, N, lmax, rd.phi0, Vp, Vm);
+        fft_stockham(buf, N, -1.0, tw);
+        gather_adjoint<SPIN, true>(buf, N, lmax, shifted, Vp, Vm);
         return;
     }
-    const int P = rd.P, Q = rd.Q, Pp = P / Q, logp = ilog2i(Pp);
+    const int P = rd.P, Q = rd.Q, Pp = P / Q;
     const double2 *B = bh + rd.bh_off;
     double2 *Wg = W_all + (size_t)blockIdx.y * npix + rd.start;
     for (int s = 0; s < Q; ++s) {
         for (int q = threadIdx.x; q < Pp; q += blockDim.x) {
             double2 v = make_double2(0.0, 0.0);
-            for (int j = q; j < N; j += Pp) {
-                double2 a = cmul(make_double2(inQ[j], SPIN ? inU[j] : 0.0), chirp(j, N, -1.0));
-                if (s) a = cmul(a, root((long long)s * j, P, -1.0));
-                v = cadd(v, a);
-            }
-            buf[brev(q, logp)] = v;
+            for (int j = q; j < N; j += Pp)
+                v = cadd(v, cmul(make_double2(inQ[j], SPIN ? inU[j] : 0.0), cis_pi(-((j * j) % (2 * N)), N, -s * j, P)));
+            buf[pidx(q)] = v;
         }
         __syncthreads();
-        fft_smem(buf, Pp, -1, tw);
-        for (int q = threadIdx.x; q < Pp; q += blockDim.x) buf[q] = cmul(buf[q], bh_get(B, P, Q * q + s, -1));
+        fft_stockham(buf, Pp, -1.0, tw);
+        for (int q = threadIdx.x; q < Pp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, P, Q * q + s, -1));
         __syncthreads();
-        fft_smem_dif(buf, Pp, +1, tw);  // output in bit-reversed order
+        fft_stockham(buf, Pp, +1.0, tw);
         // W[k] = w'(k) conv[k], accumulated over the pieces in the ring's slot of the scratch
         for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            double2 v = buf[brev(k & (Pp - 1), logp)];
-            if (s) v = cmul(v, root((long long)s * k, P, 1.0));
-            v = cmul(v, chirp(k, N, -1.0));
+            const double2 v = cmul(buf[pidx(k & (Pp - 1))], cis_pi(-((k * k) % (2 * N)), N, s * k, P));
             Wg[k] = s ? cadd(Wg[k], v) : v;
         }
         __syncthreads();
     }
     __threadfence_block();
-    gather_adjoint<SPIN>(Wg, N, lmax, rd.phi0, Vp, Vm);
+    gather_adjoint<SPIN, false>(Wg, N, lmax, shifted, Vp, Vm);
 }
 
 // One block per (Bluestein length, piece): Bh+[Q q + s] = (1/P) sum_n b[n] e^{-2 pi i (Qq+s) n / P}.
@@ -258,7 +367,7 @@ __global__ void __launch_bounds__(kFftThreads) bluestein_setup_kernel(const int 
     const int Q = P > kFftMax ? P / kFftMax : 1;
     const int s = blockIdx.y;
     if (s >= Q) return;
-    const int Pp = P / Q, logp = ilog2i(Pp);
+    const int Pp = P / Q;
     double2 *out = bh + offs[blockIdx.x];
     for (int q = threadIdx.x; q < Pp; q += blockDim.x) {
         double2 v = make_double2(0.0, 0.0);
@@ -272,16 +381,18 @@ __global__ void __launch_bounds__(kFftThreads) bluestein_setup_kernel(const int 
             if (s) b = cmul(b, root((long long)s * idx, P, -1.0));
             v = cadd(v, b);
         }
-        buf[brev(q, logp)] = v;
+        buf[pidx(q)] = v;
     }
     __syncthreads();
-    fft_smem(buf, Pp, -1, tw);
+    fft_stockham(buf, Pp, -1.0, tw);
     const double inv = 1.0 / (double)P;
-    for (int q = threadIdx.x; q < Pp; q += blockDim.x)
-        out[(long long)Q * q + s] = make_double2(buf[q].x * inv, buf[q].y * inv);
+    for (int q = threadIdx.x; q < Pp; q += blockDim.x) {
+        const double2 v = buf[pidx(q)];
+        out[(long long)Q * q + s] = make_double2(v.x * inv, v.y * inv);
+    }
 }
 
-int smem_bytes() { return kFftMax * (int)sizeof(double2); }
+int smem_bytes() { return kFftBufLen * (int)sizeof(double2); }
 
 template <typename K>
 int ensure_smem(K kernel) {
