@@ -9,6 +9,12 @@ loss copied out every step.  Kernel time is measured live with CUDA events aroun
 each stage launch inside the C ABI (jhtb_plan_set_timing); the FP64 roofline
 denominator is measured with the in-library FMA probe.
 
+``mixed`` is the batched mixed-precision form of the same step: B maps per step,
+the synthesis on the tensor cores (split-BF16 products, FP32 accumulation folded
+into FP64), the VJP's adjoint and the ring transforms in FP64; it reports maps/s,
+the ratio to the FP64 maps/s, and the relative error of every map and gradient
+against the FP64 path on the same inputs.
+
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
 With torchrun (N > 1) every rank transforms its own maps (independent work, no
@@ -49,6 +55,8 @@ def parse_args():
     ap.add_argument("--lmax", type=int, default=4096)
     ap.add_argument("--cpu-sample-m", type=int, default=48, help="orders in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-batch", type=int, default=8, help="maps per step of the mixed-precision form (0: skip)")
+    ap.add_argument("--mixed-steps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -191,6 +199,69 @@ def dist_setup(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def run_mixed(args, jhtb, _lib, torch, dev, pg, nside, lmax, spin, rank, world, fp64_ms_per_step):
+    """Batched mixed-precision step: B maps of synthesis (tensor cores) + VJP (FP64 adjoint)."""
+    B = args.mixed_batch
+    alm = np.stack([make_inputs(5000 + 97 * rank + b, nside, lmax)[0] for b in range(B)])
+    rng = np.random.default_rng(77 + rank)
+    a = torch.as_tensor(alm, device=dev).requires_grad_(True)
+    d = torch.as_tensor(rng.standard_normal((B, 2, 12 * nside * nside)), device=dev)
+
+    def step(prec):
+        a.grad = None
+        m = jhtb.synthesis_batch(a, nside, lmax, spin, precision=prec)
+        loss = 0.5 * torch.sum((m - d) ** 2)
+        loss.backward()
+        return m.detach(), a.grad.detach().clone()
+
+    # error of every map and gradient against the FP64 path on the same inputs
+    m64, g64 = step("fp64")
+    mmx, gmx = step("bf16x3")
+    torch.cuda.synchronize()
+    den_m = torch.amax(torch.abs(m64).reshape(B, -1), dim=1)
+    err_m = torch.amax(torch.abs(mmx - m64).reshape(B, -1), dim=1) / den_m
+    den_g = torch.amax(torch.abs(g64).reshape(B, -1), dim=1)
+    err_g = torch.amax(torch.abs(gmx - g64).reshape(B, -1), dim=1) / den_g
+    del m64, g64, mmx, gmx
+    plan = _lib.get_plan(nside, lmax, spin, "bf16x3", B)
+    for _ in range(max(1, args.warmup - 1)):
+        step("bf16x3")
+    torch.cuda.synchronize()
+    plan.timings(reset=True)
+    if pg:
+        pg.barrier()
+    plan.set_timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.mixed_steps):
+        step("bf16x3")
+    e1.record()
+    torch.cuda.synchronize()
+    plan.set_timing(False)
+    dev_ms = e0.elapsed_time(e1)
+    stage = plan.timings(reset=True)
+    if pg:
+        t = torch.tensor([dev_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    ms_step = dev_ms / args.mixed_steps
+    value = world * B / (ms_step * 1e-3)
+    fp64_value = world / (fp64_ms_per_step * 1e-3)
+    return {
+        "value": value,
+        "unit": UNIT,
+        "maps_per_step_per_gpu": B,
+        "ms_per_step": ms_step,
+        "vs_fp64_plain": value / fp64_value,
+        "precision": "synthesis bf16x3 (tensor cores, FP32 block sums folded into FP64); adjoint and ring FFTs FP64",
+        "rel_err_synthesis_vs_fp64": {"max": float(err_m.max()), "per_map": [float(e) for e in err_m]},
+        "rel_err_gradient_vs_fp64": {"max": float(err_g.max()), "per_map": [float(e) for e in err_g]},
+        "avg_launch_ms": {k: v / max(n, 1) for k, (v, n) in stage.items()},
+        "gpu_launches": sum(n for _, n in stage.values()),
+    }
 
 
 def main():
@@ -336,13 +407,18 @@ def main():
     leg_a_ms, leg_a_n = stage["legendre_adjoint"]
     avg_s = leg_s_ms / max(leg_s_n, 1)
     avg_a = leg_a_ms / max(leg_a_n, 1)
-    achieved = flops_per_launch / (avg_s * 1e-3) / 1e12
+    achieved = flops_per_launch / (avg_a * 1e-3) / 1e12  # the adjoint is the longest launch
     traffic = None
-    prof = ROOT / "profiles" / "legendre_synth2_n2048_l4096.md"
+    prof = ROOT / "profiles" / "legendre_adjoint2_n2048_l4096.md"
     if prof.exists():
         mt = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", prof.read_text())
         if mt:
             traffic = float(mt.group(1))
+
+    # ---- batched mixed precision: tensor-core synthesis, FP64 adjoint ------------------
+    mixed = None
+    if args.mixed_batch > 0:
+        mixed = run_mixed(args, jhtb, _lib, torch, dev, pg, nside, lmax, spin, rank, world, ms_per_step)
 
     if rank != 0:
         if pg:
@@ -374,7 +450,7 @@ def main():
             "parallelism": f"independent maps per GPU x{world}",
         },
         "roofline": {
-            "kernel": "legendre_synth (spin 2, FP64 fused recursion + contraction)",
+            "kernel": "legendre_adjoint (adj2_kernel: spin 2, FP64 fused recursion + ring contraction)",
             "bound": "fp64",
             "achieved": achieved,
             "peak": fp64_peak,
@@ -387,8 +463,9 @@ def main():
             "avg_launch_ms": {"legendre_synth": avg_s, "legendre_adjoint": avg_a,
                               "ring_synth": stage["ring_synth"][0] / max(stage["ring_synth"][1], 1),
                               "ring_adjoint": stage["ring_adjoint"][0] / max(stage["ring_adjoint"][1], 1)},
-            "adjoint_frac": flops_per_launch / (avg_a * 1e-3) / 1e12 / fp64_peak,
+            "synthesis_frac": flops_per_launch / (avg_s * 1e-3) / 1e12 / fp64_peak,
         },
+        "mixed": mixed,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": sum(n for _, n in stage.values()),
         "clocks": clocks,
