@@ -127,6 +127,22 @@ int jhtb_dot(const jhtb_plan *plan, int64_t n, const double *x, const double *y,
  * on each device looks up the array's address; make it before any stream capture. */
 int jhtb_synthesis_noalloc(int nside, int lmax, const void *alm, void *map, void *stream);
 
+/* ---- sharding over devices (no counterpart in jht, which runs on one device) ----
+ * A plan can be restricted to the ring pairs of half-grid rings [t0, t1) (the
+ * northern rings t0..t1-1, the equator included when t1 = 2 nside, and their
+ * southern mirrors).  Synthesis then writes only the pixels of those rings (other
+ * pixels of the output are left as they were) and the adjoint returns only their
+ * contribution, so the adjoints of plans whose ranges cover [0, 2 nside) once sum to
+ * the full adjoint.  Ranges are aligned to 256 rings. */
+
+/* Legendre work of each group of `granule` half-grid rings (granule a positive
+ * multiple of 256), in ring-recursion steps: cost[g] for g < ceil(2 nside / granule). */
+int jhtb_plan_ring_costs(const jhtb_plan *plan, int granule, int64_t *cost, int ncost);
+
+/* Restrict the plan to half-grid rings [t0, t1): 0 <= t0 < t1 <= 2 nside, t0 and t1
+ * multiples of 256 (t1 may be 2 nside).  Synchronises the device. */
+int jhtb_plan_set_ring_range(jhtb_plan *plan, int t0, int t1);
+
 /* ---- diagnostics (no counterpart in jht; its profiling is by stage-timing scripts,
  * scripts/profile_adjoint.py) ---------------------------------------------------- */
 

@@ -43,6 +43,8 @@ EXPORTS = (
     "jhtb_probe_fp64_fma",
     "jhtb_synthesis_noalloc",
     "jhtb_plan_status",
+    "jhtb_plan_ring_costs",
+    "jhtb_plan_set_ring_range",
 )
 
 
@@ -96,6 +98,8 @@ def load_library(path: str | os.PathLike | None = None):
                                          ctypes.POINTER(ctypes.c_double), vp]),
             "jhtb_synthesis_noalloc": (i32, [i32, i32, vp, vp, vp]),
             "jhtb_plan_status": (i32, [vp, ctypes.POINTER(i32)]),
+            "jhtb_plan_ring_costs": (i32, [vp, i32, ctypes.POINTER(i64), i32]),
+            "jhtb_plan_set_ring_range": (i32, [vp, i32, i32]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -204,6 +208,17 @@ class Plan:
         e = ctypes.c_int()
         check(self.lib.jhtb_plan_status(self.handle, ctypes.byref(e)), "jhtb_plan_status")
         return int(e.value)
+
+    def ring_costs(self, granule: int = 256) -> np.ndarray:
+        """Legendre work (ring-recursion steps) of each group of `granule` half-grid rings."""
+        n = (2 * self.nside + granule - 1) // granule
+        out = (ctypes.c_int64 * n)()
+        check(self.lib.jhtb_plan_ring_costs(self.handle, granule, out, n), "jhtb_plan_ring_costs")
+        return np.array(out[:], dtype=np.int64)
+
+    def set_ring_range(self, t0: int, t1: int) -> None:
+        """Restrict the plan to half-grid rings [t0, t1) and their southern mirrors."""
+        check(self.lib.jhtb_plan_set_ring_range(self.handle, int(t0), int(t1)), "jhtb_plan_set_ring_range")
 
     def set_timing(self, enable: bool) -> None:
         check(self.lib.jhtb_plan_set_timing(self.handle, int(enable)), "jhtb_plan_set_timing")

@@ -123,6 +123,15 @@ struct Plan {
     bool tc_owns_tables;
     int *d_err;           // device error flag
 
+    // ring-pair range of the plan (sharding over devices): half-grid rings
+    // [ring_t0, ring_t1) and their southern mirrors; the whole grid by default
+    int ring_t0, ring_t1;
+    int nsynth;           // entries of d_synth_order (items inside the range)
+    int tc_norder;        // entries of d_tc_order
+    int *d_ring_list;     // [nring_list] ring indices of the range, or null for all rings
+    int nring_list;
+    std::vector<int> h_lw, h_tc_lw;  // start l per item, kept for re-sorting
+
     // workspace
     double2 *d_F;       // [chunk][nchan][nrings][M] ring spectra
     double2 *d_W;       // [chunk][npix] Bluestein accumulation scratch (adjoint, Q > 1)
@@ -152,6 +161,7 @@ int launch_start_states_r(const Plan &p, int R, int ntiles, int *lw, double2 *st
 int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaStream_t s);
 int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *offs, int nlen,
                            cudaStream_t s);
+constexpr int kRingGranule = 256;  // alignment of ring ranges: a multiple of every tile width
 
 __host__ __device__ inline long long alm_index(long long l, long long m, long long lmax) {
     return m * (2 * lmax + 1 - m) / 2 + l;

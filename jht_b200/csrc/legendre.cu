@@ -57,6 +57,7 @@ struct LegParams {
     const double *alpha, *gamma, *cnorm;
     // work items
     int ntiles;               // warp tiles per m
+    int nsynth;               // entries of synth_order
     int nsuper, tps;          // adjoint: quarters per m, warp tiles per quarter
     const int *lw;            // [M * ntiles] start l per (m, tile)
     const double2 *st;        // [M * ntiles][nrec][R][32] start (u1, u2)
@@ -84,6 +85,7 @@ LegParams make_params(const Plan &p) {
     q.gamma = p.d_gamma;
     q.cnorm = p.d_cnorm;
     q.ntiles = p.ntiles;
+    q.nsynth = p.nsynth;
     q.nsuper = p.nsuper;
     q.tps = p.tps;
     q.lw = p.d_lw;
@@ -295,7 +297,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth0_kernel(LegParams p
     __shared__ Stage0 stage[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     Stage0 &sb = stage[threadIdx.x >> 5];
-    const int nitems = p.M * p.ntiles;
+    const int nitems = p.nsynth;
     const int L = p.lmax;
     for (;;) {
         const int it = next_item(p.counter);
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth2_kernel(LegParams p
     __shared__ Stage2 stage[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     Stage2 &sb = stage[threadIdx.x >> 5];
-    const int nitems = p.M * p.ntiles;
+    const int nitems = p.nsynth;
     const int L = p.lmax;
     for (;;) {
         const int it = next_item(p.counter);

@@ -86,7 +86,7 @@ void free_plan(Plan *p) {
     void *ptrs[] = {p->d_x,     p->d_logsin, p->d_logch, p->d_logsh,   p->d_rings, p->d_tw,
                     p->d_bh,    p->d_seed,   p->d_alpha, p->d_gamma,   p->d_cnorm, p->d_F,
                     p->d_W,     p->d_scratch, p->d_lw, p->d_st, p->d_stsc, p->d_synth_order,
-                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err};
+                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err, p->d_ring_list};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (p->tc_owns_tables) {
@@ -99,6 +99,82 @@ void free_plan(Plan *p) {
         cudaEventDestroy(e.stop);
     }
     delete p;
+}
+
+// Cost-sorted item orders of the persistent kernels, restricted to the items whose
+// tile lies inside the plan's ring range, and the ring list of the azimuthal stage.
+// Called at plan creation and again whenever the range changes.
+int build_orders(Plan *p) {
+    const int L = p->lmax, M = p->M, T = p->T;
+    const int t0 = p->ring_t0, t1 = p->ring_t1;
+    size_t bytes = 0;
+    auto refresh = [&](int **dptr, const std::vector<int> &h) -> int {
+        if (*dptr) cudaFree(*dptr);
+        *dptr = nullptr;
+        return upload(dptr, h, bytes);
+    };
+    int rc;
+    // FP64 kernels: tiles of 32 R rings
+    {
+        const int tw = 32 * (p->spin ? kR2 : kR0);
+        const std::vector<int> &lw = p->h_lw;
+        auto in_range = [&](int tile) { return tile * tw >= t0 && tile * tw < t1; };
+        auto cost = [&](long long it) { return std::max(0, L + 1 - lw[it]); };
+        std::vector<int> so;
+        for (long long i = 0; i < (long long)M * p->ntiles; ++i)
+            if (in_range((int)(i % p->ntiles))) so.push_back((int)i);
+        std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return cost(a) > cost(b); });
+        const long long nsup = (long long)M * p->nsuper;
+        std::vector<int> at((size_t)nsup * p->tps, -1), ao(nsup);
+        std::vector<long long> acost(nsup, 0);
+        for (int m = 0; m < M; ++m)
+            for (int s = 0; s < p->nsuper; ++s) {
+                std::vector<int> tl;
+                for (int t = s * p->tps; t < std::min((s + 1) * p->tps, p->ntiles); ++t)
+                    if (in_range(t)) tl.push_back(t);
+                std::stable_sort(tl.begin(), tl.end(), [&](int a, int b) {
+                    return lw[(long long)m * p->ntiles + a] < lw[(long long)m * p->ntiles + b];
+                });
+                const long long si = (long long)m * p->nsuper + s;
+                for (size_t j = 0; j < tl.size(); ++j) {
+                    at[si * p->tps + j] = tl[j];
+                    acost[si] += cost((long long)m * p->ntiles + tl[j]);
+                }
+                ao[si] = (int)si;
+            }
+        std::stable_sort(ao.begin(), ao.end(), [&](int a, int b) { return acost[a] > acost[b]; });
+        p->nsynth = (int)so.size();
+        if ((rc = refresh(&p->d_synth_order, so))) return rc;
+        if ((rc = refresh(&p->d_adj_order, ao))) return rc;
+        if ((rc = refresh(&p->d_adj_tiles, at))) return rc;
+    }
+    // tensor-core kernel: tiles of 128 (spin 2) or 256 (spin 0) rings
+    if (p->precision == JHTB_PREC_BF16X3) {
+        const int tw = p->spin ? 128 : 256;
+        const std::vector<int> &lw = p->h_tc_lw;
+        std::vector<int> so;
+        for (long long i = 0; i < (long long)M * p->tc_ntiles; ++i) {
+            const int tile = (int)(i % p->tc_ntiles);
+            if (tile * tw >= t0 && tile * tw < t1) so.push_back((int)i);
+        }
+        std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return lw[a] < lw[b]; });
+        p->tc_norder = (int)so.size();
+        if ((rc = refresh(&p->d_tc_order, so))) return rc;
+    }
+    // azimuthal stage: the range's northern rings and their southern mirrors
+    if (p->d_ring_list) cudaFree(p->d_ring_list);
+    p->d_ring_list = nullptr;
+    p->nring_list = 0;
+    if (t0 != 0 || t1 != T) {
+        std::vector<int> rl;
+        for (int t = t0; t < t1; ++t) {
+            rl.push_back(t);
+            if (t < T - 1) rl.push_back(4 * p->nside - 2 - t);
+        }
+        p->nring_list = (int)rl.size();
+        if ((rc = upload(&p->d_ring_list, rl, bytes))) return rc;
+    }
+    return JHTB_OK;
 }
 
 int build_plan(Plan *p, const jhtb_host_tables *ht) {
@@ -229,33 +305,8 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nst_el + 4 * sizeof(unsigned);
         if ((rc = launch_start_states(*p, 0))) return rc;
         JHTB_CUDA_TRY(cudaDeviceSynchronize());
-        std::vector<int> lw(nitems);
-        JHTB_CUDA_TRY(cudaMemcpy(lw.data(), p->d_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
-        auto cost = [&](long long it) { return std::max(0, L + 1 - lw[it]); };
-        std::vector<int> so(nitems);
-        for (long long i = 0; i < nitems; ++i) so[i] = (int)i;
-        std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return cost(a) > cost(b); });
-        const long long nsup = (long long)M * p->nsuper;
-        std::vector<int> at((size_t)nsup * p->tps, -1), ao(nsup);
-        std::vector<long long> acost(nsup, 0);
-        for (int m = 0; m < M; ++m)
-            for (int s = 0; s < p->nsuper; ++s) {
-                std::vector<int> tl;
-                for (int t = s * p->tps; t < std::min((s + 1) * p->tps, p->ntiles); ++t) tl.push_back(t);
-                std::stable_sort(tl.begin(), tl.end(), [&](int a, int b) {
-                    return lw[(long long)m * p->ntiles + a] < lw[(long long)m * p->ntiles + b];
-                });
-                const long long si = (long long)m * p->nsuper + s;
-                for (size_t j = 0; j < tl.size(); ++j) {
-                    at[si * p->tps + j] = tl[j];
-                    acost[si] += cost((long long)m * p->ntiles + tl[j]);
-                }
-                ao[si] = (int)si;
-            }
-        std::stable_sort(ao.begin(), ao.end(), [&](int a, int b) { return acost[a] > acost[b]; });
-        if ((rc = upload(&p->d_synth_order, so, bytes))) return rc;
-        if ((rc = upload(&p->d_adj_order, ao, bytes))) return rc;
-        if ((rc = upload(&p->d_adj_tiles, at, bytes))) return rc;
+        p->h_lw.resize(nitems);
+        JHTB_CUDA_TRY(cudaMemcpy(p->h_lw.data(), p->d_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
     }
 
     // ---- tensor-core path: 128-ring tiles ---------------------------------------------------
@@ -276,12 +327,12 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nel;
         if ((rc = launch_start_states_r(*p, Rt, p->tc_ntiles, p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, 0))) return rc;
         JHTB_CUDA_TRY(cudaDeviceSynchronize());
-        std::vector<int> lw(nitems), so(nitems);
-        JHTB_CUDA_TRY(cudaMemcpy(lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
-        for (long long i = 0; i < nitems; ++i) so[i] = (int)i;
-        std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return lw[a] < lw[b]; });
-        if ((rc = upload(&p->d_tc_order, so, bytes))) return rc;
+        p->h_tc_lw.resize(nitems);
+        JHTB_CUDA_TRY(cudaMemcpy(p->h_tc_lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
     }
+    p->ring_t0 = 0;
+    p->ring_t1 = T;
+    if ((rc = build_orders(p))) return rc;
 
     // ---- ring FFT descriptors -------------------------------------------------------------
     std::vector<RingDesc> rings(nr);
@@ -508,6 +559,37 @@ int jhtb_plan_status(jhtb_plan *plan, int *device_error) {
     JHTB_CUDA_TRY(cudaMemcpy(device_error, p.d_err, sizeof(int), cudaMemcpyDeviceToHost));
     JHTB_CUDA_TRY(cudaMemset(p.d_err, 0, sizeof(int)));
     return JHTB_OK;
+}
+
+int jhtb_plan_ring_costs(const jhtb_plan *plan, int granule, int64_t *cost, int ncost) {
+    if (!plan || !cost) return fail(JHTB_ERR_INVALID, "jhtb_plan_ring_costs: NULL argument");
+    const Plan &p = *reinterpret_cast<const Plan *>(plan);
+    if (granule <= 0 || granule % kRingGranule)
+        return fail(JHTB_ERR_INVALID, "jhtb_plan_ring_costs: granule must be a positive multiple of " +
+                                          std::to_string(kRingGranule));
+    const int ng = (p.T + granule - 1) / granule;
+    if (ncost < ng) return fail(JHTB_ERR_INVALID, "jhtb_plan_ring_costs: need " + std::to_string(ng) + " entries");
+    for (int g = 0; g < ng; ++g) cost[g] = 0;
+    const int tw = 32 * (p.spin ? kR2 : kR0);
+    for (long long i = 0; i < (long long)p.M * p.ntiles; ++i) {
+        const int tile = (int)(i % p.ntiles);
+        const int t_lo = tile * tw, t_hi = std::min(p.T, t_lo + tw);
+        cost[t_lo / granule] += (int64_t)std::max(0, p.lmax + 1 - p.h_lw[i]) * (t_hi - t_lo);
+    }
+    return JHTB_OK;
+}
+
+int jhtb_plan_set_ring_range(jhtb_plan *plan, int t0, int t1) {
+    if (!plan) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_ring_range: NULL plan");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    if (t0 < 0 || t1 > p.T || t0 >= t1 || t0 % kRingGranule || (t1 % kRingGranule && t1 != p.T))
+        return fail(JHTB_ERR_INVALID, "jhtb_plan_set_ring_range: need 0 <= t0 < t1 <= 2 nside = " +
+                                          std::to_string(p.T) + " with t0 and t1 (unless 2 nside) multiples of " +
+                                          std::to_string(kRingGranule));
+    JHTB_CUDA_TRY(cudaDeviceSynchronize());  // no launch of this plan may still read the old orders
+    p.ring_t0 = t0;
+    p.ring_t1 = t1;
+    return build_orders(&p);
 }
 
 int jhtb_plan_set_timing(jhtb_plan *plan, int enable) {

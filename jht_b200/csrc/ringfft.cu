@@ -224,14 +224,15 @@ __device__ __forceinline__ double2 fold_synth(const double2 *__restrict__ Fp, co
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, 1) ring_synth_kernel(const RingDesc *__restrict__ rings, int lmax,
+__global__ void __launch_bounds__(kFftThreads, 1) ring_synth_kernel(const int *__restrict__ ring_list,
+                                                                     const RingDesc *__restrict__ rings, int lmax,
                                                                   int M, int nrings, long long npix,
                                                                   const double2 *__restrict__ F_all,
                                                                   double *__restrict__ maps_all,
                                                                   const double2 *__restrict__ tw,
                                                                   const double2 *__restrict__ bh) {
     extern __shared__ double2 buf[];
-    const int r = blockIdx.x;
+    const int r = ring_list ? ring_list[blockIdx.x] : (int)blockIdx.x;
     const RingDesc rd = rings[r];
     const int N = rd.N;
     const bool shifted = rd.phi0 != 0.0;
@@ -305,7 +306,8 @@ __device__ __forceinline__ void gather_adjoint(const double2 *W, int N, int lmax
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, 1) ring_adjoint_kernel(const RingDesc *__restrict__ rings, int lmax,
+__global__ void __launch_bounds__(kFftThreads, 1) ring_adjoint_kernel(const int *__restrict__ ring_list,
+                                                                       const RingDesc *__restrict__ rings, int lmax,
                                                                     int M, int nrings, long long npix,
                                                                     const double *__restrict__ maps_all,
                                                                     double2 *__restrict__ V_all,
@@ -313,7 +315,7 @@ __global__ void __launch_bounds__(kFftThreads, 1) ring_adjoint_kernel(const Ring
                                                                     const double2 *__restrict__ tw,
                                                                     const double2 *__restrict__ bh) {
     extern __shared__ double2 buf[];
-    const int r = blockIdx.x;
+    const int r = ring_list ? ring_list[blockIdx.x] : (int)blockIdx.x;
     const RingDesc rd = rings[r];
     const int N = rd.N;
     const bool shifted = rd.phi0 != 0.0;
@@ -404,15 +406,15 @@ int ensure_smem(K kernel) {
 
 int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;
-    dim3 grid(p.nrings, nb);
+    dim3 grid(p.d_ring_list ? p.nring_list : p.nrings, nb);
     int rc;
     if (p.spin == 0) {
         if ((rc = ensure_smem(ring_synth_kernel<0>))) return rc;
-        ring_synth_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
+        ring_synth_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
                                                                      maps, p.d_tw, p.d_bh);
     } else {
         if ((rc = ensure_smem(ring_synth_kernel<2>))) return rc;
-        ring_synth_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
+        ring_synth_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
                                                                      maps, p.d_tw, p.d_bh);
     }
     JHTB_CUDA_TRY(cudaGetLastError());
@@ -421,15 +423,15 @@ int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cud
 
 int launch_ring_adjoint(const Plan &p, const double *maps, double2 *V, double2 *W, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;
-    dim3 grid(p.nrings, nb);
+    dim3 grid(p.d_ring_list ? p.nring_list : p.nrings, nb);
     int rc;
     if (p.spin == 0) {
         if ((rc = ensure_smem(ring_adjoint_kernel<0>))) return rc;
-        ring_adjoint_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_rings, p.lmax, p.M, p.nrings, p.npix,
+        ring_adjoint_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix,
                                                                        maps, V, W, p.d_tw, p.d_bh);
     } else {
         if ((rc = ensure_smem(ring_adjoint_kernel<2>))) return rc;
-        ring_adjoint_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_rings, p.lmax, p.M, p.nrings, p.npix,
+        ring_adjoint_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix,
                                                                        maps, V, W, p.d_tw, p.d_bh);
     }
     JHTB_CUDA_TRY(cudaGetLastError());

@@ -89,13 +89,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return false;
 }
 
-__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
-            d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
-        : "memory");
-}
 // A operand from tensor memory (ts form), B from a shared-memory descriptor.
 __device__ __forceinline__ void umma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
                                             uint32_t acc) {
@@ -123,13 +116,6 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
-                 "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-                 "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-                 "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
-                 : "memory");
 }
 __device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(a), "r"(b), "r"(c),
@@ -206,6 +192,7 @@ struct TcParams {
     const SeedParam *seed;
     const double *alpha, *gamma, *cnorm;
     int ntiles;  // item tiles per m (128 rings for spin 2, 256 for spin 0)
+    int norder;  // entries of order (the items inside the plan's ring range)
     const int *lw;
     const double2 *st;
     const int *stsc;
@@ -376,7 +363,7 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
     const int row = warp * 32 + lane;  // A row = TMEM lane
     const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16);
     float(&acc)[2][C::NG][N][kTcRows] = sm.acc;
-    const int nitems = p.M * p.ntiles;
+    const int nitems = p.norder;
     const int total = nitems * ((nb + BM - 1) / BM);
     const int stride = gridDim.x;
     unsigned gc = 0, bk = 0;
@@ -575,7 +562,7 @@ __device__ void tc_builder(const TcParams &p, const double2 *__restrict__ alm_al
     using C = TcCfg<SPIN, BM>;
     const int k = bt % kTcK, bm = bt / kTcK;
     const double sg = (k & 1) ? -1.0 : 1.0;  // (-1)^(l - lmin): chunks start at even offsets
-    const int nitems = p.M * p.ntiles;
+    const int nitems = p.norder;
     // the loads run two chunks ahead of the stores
     TcCursor<BM> ld{(int)blockIdx.x, 0, nitems * ((nb + BM - 1) / BM), nitems, nb, TcItem{}};
     ld.settle(p);
@@ -631,7 +618,7 @@ __device__ void tc_mma(const TcParams &p, TcSmem<SPIN, BM> &sm, int nb, uint32_t
     using C = TcCfg<SPIN, BM>;
     constexpr int N = C::N;
     constexpr uint32_t IDESC = idesc_bf16(kTcRows, N);
-    const int nitems = p.M * p.ntiles;
+    const int nitems = p.norder;
     const int total = nitems * ((nb + BM - 1) / BM);
     unsigned gc = 0, bk = 0;
     bool ok = true;
@@ -784,6 +771,7 @@ int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaS
     q.st = p.d_tc_st;
     q.stsc = p.d_tc_stsc;
     q.order = p.d_tc_order;
+    q.norder = p.tc_norder;
     q.err = p.d_err;
     return p.spin ? launch_tc_synth_t<2>(q, alm, F, nb, s) : launch_tc_synth_t<0>(q, alm, F, nb, s);
 }
