@@ -23,9 +23,9 @@
 //     (kind::f16, A from tensor memory, B from shared memory, FP32 accumulators in
 //     tensor memory) and commits each stage back to its producers.
 // hh accumulates apart from the five smaller products (relative size <= 2^-8).
-// Every kFlush chunks (128 l) the producers fold the FP32 block sums into per-thread
+// Every kFlush chunks (256 l) the producers fold the FP32 block sums into per-thread
 // double-float (hi, lo) accumulators in shared memory, so FP32 rounding acts on at
-// most 128 terms; the item's result is hi + lo in FP64.  Every wait is bounded; on
+// most 256 terms; the item's result is hi + lo in FP64.  Every wait is bounded; on
 // timeout the kernel records an error, every role leaves its loop, and tensor memory
 // is released after the last MMA has drained.
 #include <cuda_bf16.h>
@@ -40,7 +40,7 @@ namespace {
 
 constexpr int kTcRows = 128;     // = MMA M = rings per tile
 constexpr int kTcK = 16;         // l steps per chunk = MMA K (BF16)
-constexpr int kFlush = 8;        // chunks per FP32 accumulation block
+constexpr int kFlush = 16;       // chunks per FP32 accumulation block (256 l)
 constexpr unsigned kWaitLimit = 1u << 26;
 
 // ---------------------------------------------------------------------------------
