@@ -8,8 +8,7 @@ signatures and conventions, running hand-written CUDA kernels through the
     m = jht.synthesis(alm, nside, lmax, spin=0)        # a_lm -> map
     a = jht.analysis(m, nside, lmax, spin=0, niter=3)  # map -> a_lm
 
-Out of scope here (not provided): the off-grid NUFFT transforms, ``wiener`` and
-``constrained_realization``.
+Out of scope here (not provided): the off-grid NUFFT transforms.
 """
 
 from __future__ import annotations
@@ -26,7 +25,17 @@ from .healpix import (
     synthesis,
     synthesis_batch,
 )
-from .masked import alm_to_real, deconvolve, deconvolve_batch, n_dof, pseudo_alm, real_to_alm
+from .masked import (
+    alm_to_real,
+    constrained_realization,
+    deconvolve,
+    deconvolve_batch,
+    n_dof,
+    pseudo_alm,
+    real_to_alm,
+    wiener,
+    wiener_batch,
+)
 from .weights import pixel_weights, ring_weights
 
 __version__ = "0.1.0"
@@ -42,6 +51,8 @@ __all__ = [
     "pixel_weights",
     "pseudo_alm",
     "deconvolve",
+    "wiener",
+    "constrained_realization",
     "synthesis_real",
     "analysis_real",
     "bandpower",
@@ -58,4 +69,5 @@ __all__ = [
     "synthesis_batch",
     "adjoint_synthesis_batch",
     "deconvolve_batch",
+    "wiener_batch",
 ]

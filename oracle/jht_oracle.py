@@ -682,6 +682,67 @@ def deconvolve(maps, mask, nside, lmax, spin=0, *, max_iter=200, tol=1e-8, reg=0
     return real_to_alm(xs, lmax, spin)
 
 
+def weight_pix(nside, spin, *, inv_noise=None, mask=None, use_weights=True):
+    """Per-pixel CG weight: N^-1 if given, else mask * W (masked.py:77-93)."""
+    if inv_noise is not None:
+        w = np.asarray(inv_noise, dtype=np.float64)
+    elif mask is not None:
+        w = np.asarray(mask, dtype=np.float64) * pixel_weights(nside, use_weights)
+    else:
+        raise ValueError("provide either inv_noise (per-pixel N^-1) or mask")
+    return w if spin == 0 else w[None, :]
+
+
+def prior_sqrt(signal_cl, lmax, spin):
+    """x-space whitening sqrt(Cl) per real DOF, exactly 0 on zero-power multipoles (masked.py:181-227)."""
+    ms, ls = [], []
+    for m in range(lmax + 1):
+        ms.append(np.full(lmax + 1 - m, m))
+        ls.append(np.arange(m, lmax + 1))
+    ms, ls = np.concatenate(ms), np.concatenate(ls)
+    act = ls >= abs(spin)
+    ell = np.concatenate([ls[act & (ms == 0)], ls[act & (ms > 0)], ls[act & (ms > 0)]])
+
+    def one(cl):
+        c = np.asarray(cl, dtype=np.float64)[ell]
+        return np.where(c > 0, np.sqrt(np.where(c > 0, c, 1.0)), 0.0)
+
+    return one(signal_cl) if spin == 0 else np.concatenate([one(signal_cl[0]), one(signal_cl[1])])
+
+
+def _whitened_system(maps, w, pw, nside, lmax, spin):
+    b = pw * alm_to_real(adjoint_synthesis(w * np.asarray(maps), nside, lmax, spin), lmax, spin)
+
+    def op(y):
+        a = real_to_alm(pw * y, lmax, spin)
+        return pw * alm_to_real(adjoint_synthesis(w * synthesis(a, nside, lmax, spin), nside, lmax, spin),
+                                lmax, spin) + y
+
+    return b, op
+
+
+def wiener(maps, signal_cl, nside, lmax, spin=0, *, inv_noise=None, mask=None, max_iter=200, tol=1e-8,
+           use_weights=True):
+    """Wiener mean: CG on (P A_x P + I) y = P b_x, a = T^-1 P y (masked.py:320-372)."""
+    w = weight_pix(nside, spin, inv_noise=inv_noise, mask=mask, use_weights=use_weights)
+    pw = prior_sqrt(signal_cl, lmax, spin)
+    b, op = _whitened_system(maps, w, pw, nside, lmax, spin)
+    y, _ = cg(op, b, tol=tol, maxiter=max_iter)
+    return real_to_alm(pw * y, lmax, spin)
+
+
+def constrained_realization(maps, signal_cl, nside, lmax, omega, xi, spin=0, *, inv_noise=None, mask=None,
+                            max_iter=200, tol=1e-8, use_weights=True):
+    """Posterior draw for given sources omega (pixel space) and xi (x space) (masked.py:375-439)."""
+    w = weight_pix(nside, spin, inv_noise=inv_noise, mask=mask, use_weights=use_weights)
+    pw = prior_sqrt(signal_cl, lmax, spin)
+    b, op = _whitened_system(maps, w, pw, nside, lmax, spin)
+    s1 = alm_to_real(adjoint_synthesis(np.sqrt(w) * np.asarray(omega), nside, lmax, spin), lmax, spin)
+    rhs = b + pw * s1 + np.where(pw > 0, np.asarray(xi), 0.0)
+    y, _ = cg(op, rhs, tol=tol, maxiter=max_iter)
+    return real_to_alm(pw * y, lmax, spin)
+
+
 def bandpower(alm, lmax: int, spin: int = 0) -> np.ndarray:
     """C_l = (2l+1)^-1 sum_m (2 - delta_m0)|a_lm|^2 (diff.py:119-138)."""
     ells, _ = lm_of_index(lmax)

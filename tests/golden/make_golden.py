@@ -164,6 +164,31 @@ def main(ref_root: str) -> None:
     out["cg/data"] = data
     out["cg/alm"] = np.asarray(jht.masked.deconvolve(data, mask, nside, lmax, 0, tol=1e-8, reg=1e-6))
 
+    # ---- Wiener filter (prior-whitened CG), spin 0 with the mask weighting and zero-power
+    #      multipoles, spin 2 with a per-pixel inverse noise ------------------------------
+    nside, lmax = 8, 12
+    rng = np.random.default_rng(5000)
+    ell = np.arange(lmax + 1)
+    cl0 = 1.0 / (ell + 10.0) ** 2
+    cl0[:2] = 0.0  # monopole and dipole pinned to zero
+    a_true = spectrum_alm(rng, lmax)
+    data = np.asarray(hp.synthesis(a_true, nside, lmax, 0)) + 1e-2 * rng.standard_normal(12 * nside**2)
+    out["wiener/s0_mask"] = mask
+    out["wiener/s0_data"] = data
+    out["wiener/s0_cl"] = cl0
+    out["wiener/s0_alm"] = np.asarray(jht.masked.wiener(data, cl0, nside, lmax, 0, mask=mask, tol=1e-10))
+    cle = 1.0 / (ell + 10.0) ** 2
+    clb = 0.1 / (ell + 10.0) ** 2
+    a2_true = np.stack([spectrum_alm(rng, lmax, 1.0, 2), spectrum_alm(rng, lmax, 0.1, 2)])
+    sigma = 1e-2 * (1.0 + 0.5 * np.abs(zpix))
+    inv_noise = mask / sigma**2
+    data2 = np.asarray(hp.synthesis(a2_true, nside, lmax, 2)) + sigma[None, :] * rng.standard_normal((2, 12 * nside**2))
+    out["wiener/s2_invn"] = inv_noise
+    out["wiener/s2_data"] = data2
+    out["wiener/s2_cl"] = np.stack([cle, clb])
+    out["wiener/s2_alm"] = np.asarray(
+        jht.masked.wiener(data2, (cle, clb), nside, lmax, 2, inv_noise=inv_noise, tol=1e-10))
+
     np.savez_compressed(HERE / "jht_golden.npz", **out)
     print(f"wrote {len(out)} arrays to {HERE / 'jht_golden.npz'}")
 

@@ -262,3 +262,16 @@ def test_bandpower_formula():
         for m in range(1, ell + 1):
             tot += 2 * abs(a[O.alm_base(m, lmax) + ell - m]) ** 2
         assert abs(cl[ell] - tot / (2 * ell + 1)) <= 1e-14 * max(tot, 1)
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_oracle_wiener_matches_golden(golden, spin):
+    if spin == 0:
+        out = O.wiener(golden["wiener/s0_data"], golden["wiener/s0_cl"], 8, 12, 0, mask=golden["wiener/s0_mask"], tol=1e-10)
+        ref = golden["wiener/s0_alm"]
+        assert np.all(out[:2] == 0)  # zero-power multipoles are pinned exactly
+    else:
+        cl = golden["wiener/s2_cl"]
+        out = O.wiener(golden["wiener/s2_data"], (cl[0], cl[1]), 8, 12, 2, inv_noise=golden["wiener/s2_invn"], tol=1e-10)
+        ref = golden["wiener/s2_alm"]
+    assert relerr(out, ref) <= 1e-12
