@@ -250,7 +250,7 @@ _plans_lock = threading.Lock()
 def workspace_bytes_per_map(nside: int, lmax: int, spin: int) -> int:
     ncomp = 1 if spin == 0 else 2
     K = (lmax + 1) * (lmax + 2) // 2
-    return 16 * (ncomp * (4 * nside - 1) * (lmax + 1) + 12 * nside * nside + 4 * ncomp * K)
+    return 16 * (ncomp * (4 * nside - 1) * (lmax + 1) + 2 * 12 * nside * nside + 4 * ncomp * K)
 
 
 def get_plan(nside: int, lmax: int, spin: int, precision: str = "fp64", batch: int = 1) -> Plan:

@@ -47,7 +47,9 @@ constexpr int kR2 = JHTB_R2;  // spin 2
 constexpr int kTcMaps = 8;    // maps per tensor-core pass (N = 4 * maps per GEMM)
 
 // FFT: largest power-of-two length handled in one CTA's shared memory.
-constexpr int kFftMax = 8192;
+constexpr int kFftMax = 8192;    // largest power-of-two ring handled by the direct path per piece plan
+constexpr int kTwLen = 32768;    // twiddle table length: every FFT and split length divides it
+constexpr int kFftPiece = 4096;  // largest FFT held in shared memory; longer ones run in pieces
 constexpr int kFftLogMax = 13;
 
 // Ring FFT modes.
@@ -55,9 +57,9 @@ enum RingMode : int { kDirect = 0, kBluestein = 1 };
 
 struct RingDesc {
     int N;          // pixels in the ring
-    int mode;       // kDirect (N a power of two <= kFftMax) or kBluestein
+    int mode;       // kDirect (N a power of two) or kBluestein
     int P;          // FFT length: N (direct) or Bluestein length (power of two >= 2N-1)
-    int Q;          // number of kFftMax-point pieces for P > kFftMax (else 1)
+    int Q;          // pieces of P / Q <= kFftPiece points (1, 2, 4 or 8)
     long long start;   // first pixel
     long long bh_off;  // offset (complex units) of this length's chirp spectrum
     double phi0;       // azimuth of the first pixel
@@ -91,7 +93,7 @@ struct Plan {
     double *d_logch;    // [T] log cos(theta/2)    (spin 2 seeds)
     double *d_logsh;    // [T] log sin(theta/2)
     RingDesc *d_rings;  // [nrings]
-    double2 *d_tw;      // [kFftMax] exp(-2 pi i k / kFftMax)
+    double2 *d_tw;      // [kTwLen] exp(-2 pi i k / kTwLen)
     double2 *d_bh;      // Bluestein chirp spectra, FFT_P(conj(w))/P, per distinct length
     long long bh_len;
 
@@ -134,7 +136,8 @@ struct Plan {
 
     // workspace
     double2 *d_F;       // [chunk][nchan][nrings][M] ring spectra
-    double2 *d_W;       // [chunk][npix] Bluestein accumulation scratch (adjoint, Q > 1)
+    double2 *d_W;       // [chunk][npix] ring scratch rows of the split transforms
+    double2 *d_W2;      // [chunk][npix] second scratch row (phased input / piece sums)
     double *d_scratch;  // small reduction scratch
     int chunk;          // maps per workspace pass
     size_t bytes;

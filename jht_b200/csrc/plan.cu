@@ -85,7 +85,7 @@ void free_plan(Plan *p) {
     if (!p) return;
     void *ptrs[] = {p->d_x,     p->d_logsin, p->d_logch, p->d_logsh,   p->d_rings, p->d_tw,
                     p->d_bh,    p->d_seed,   p->d_alpha, p->d_gamma,   p->d_cnorm, p->d_F,
-                    p->d_W,     p->d_scratch, p->d_lw, p->d_st, p->d_stsc, p->d_synth_order,
+                    p->d_W,     p->d_W2,     p->d_scratch, p->d_lw, p->d_st, p->d_stsc, p->d_synth_order,
                     p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err, p->d_ring_list};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -345,16 +345,16 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         d.N = (int)npr[r];
         d.start = start[r];
         d.phi0 = phi0[r];
-        if (is_pow2(d.N) && d.N <= kFftMax) {
+        if (is_pow2(d.N) && d.N <= 8 * kFftPiece) {
             d.mode = kDirect;
             d.P = d.N;
-            d.Q = 1;
+            d.Q = std::max(1, d.N / kFftPiece);
             d.bh_off = 0;
         } else {
             d.mode = kBluestein;
             d.P = (int)next_pow2(2LL * d.N - 1);
-            d.Q = std::max(1, d.P / kFftMax);
-            if (d.Q > 4) return fail(JHTB_ERR_UNSUPPORTED, "ring length too large (nside > 4096)");
+            d.Q = std::max(1, d.P / kFftPiece);
+            if (d.Q > 8) return fail(JHTB_ERR_UNSUPPORTED, "ring length too large (nside > 4096)");
             auto it = bh_offset.find(d.N);
             if (it == bh_offset.end()) {
                 bh_offset[d.N] = bh_len;
@@ -369,9 +369,9 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     }
     if ((rc = upload(&p->d_rings, rings, bytes))) return rc;
 
-    std::vector<double2> tw(kFftMax);
-    for (int k = 0; k < kFftMax; ++k) {
-        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)kFftMax;
+    std::vector<double2> tw(kTwLen);
+    for (int k = 0; k < kTwLen; ++k) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)kTwLen;
         tw[k] = make_double2((double)cosl(a), (double)sinl(a));
     }
     if ((rc = upload(&p->d_tw, tw, bytes))) return rc;
@@ -391,10 +391,11 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         bytes += part;
     }
     bool need_w = false;
-    for (auto &d : rings) need_w |= (d.mode == kBluestein);
+    for (auto &d : rings) need_w |= (d.mode == kBluestein || d.Q > 1);
     if (need_w) {
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_W, sizeof(double2) * (size_t)p->npix * p->chunk));
-        bytes += sizeof(double2) * (size_t)p->npix * p->chunk;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_W2, sizeof(double2) * (size_t)p->npix * p->chunk));
+        bytes += 2 * sizeof(double2) * (size_t)p->npix * p->chunk;
     }
     JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_scratch, 4096 * sizeof(double)));
     bytes += 4096 * sizeof(double);

@@ -7,12 +7,14 @@
 //   adjoint    W[k] = sum_j v[j] e^{-2 pi i jk/N};  V[m] = W[m mod N] e^{-i m phi0}
 //              (spin 2 also Vm[m] = conj(W[-m mod N]) e^{-i m phi0})
 // The fold is a gather (each k collects its own m's), never a scatter.  Power-of-two
-// rings up to 8192 use an in-place Stockham FFT in shared memory (radix-16 passes held
-// in registers, natural order in and out, a padded layout against bank conflicts);
-// every other length uses
+// rings use an in-place Stockham FFT in shared memory (radix-16 passes held in
+// registers, natural order in and out, a padded layout against bank conflicts), in
+// Q = N / 4096 pieces by output residue when N > 4096 (the 4 nside belt rings at
+// nside >= 2048), so a CTA needs 70 KB of shared memory and two fit on an SM; every
+// other length uses
 // Bluestein's chirp-z with an exact (n^2 mod 2N) chirp argument (_azimuth.py:150-191)
-// at a power-of-two length P >= 2N-1, split into Q = P/8192 shared-memory pieces when
-// P > 8192 (decimation in frequency on the input, twiddled recombination on the output).
+// at a power-of-two length P >= 2N-1, split into Q = P/4096 shared-memory pieces when
+// P > 4096 (decimation in frequency on the input, twiddled recombination on the output).
 #include <cuda_runtime.h>
 
 #include "jhtb_internal.cuh"
@@ -20,7 +22,7 @@
 namespace jhtb {
 namespace {
 
-constexpr int kFftThreads = 512;
+constexpr int kFftThreads = 256;
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -63,10 +65,19 @@ __device__ __forceinline__ double2 root(long long a, long long b, double sgn) {
     return make_double2(c, s);
 }
 
+// e^{-+2 pi i a / L} from the twiddle table (e^{-2 pi i j / kTwLen}), L a power of two
+// dividing kTwLen; `plus` selects the + sign.
+__device__ __forceinline__ double2 twid(const double2 *__restrict__ tw, int a, int L, bool plus) {
+    int r = a & (L - 1);
+    double2 w = __ldg(&tw[r * (kTwLen / L)]);
+    if (plus) w.y = -w.y;
+    return w;
+}
+
 // Shared-memory layout of an FFT buffer: one pad slot every 16 and every 256 elements,
 // so the strided accesses of the Stockham passes spread over the banks.
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4) + (i >> 8); }
-constexpr int kFftBufLen = kFftMax + kFftMax / 16 + kFftMax / 256;
+constexpr int kFftBufLen = kFftPiece + kFftPiece / 16 + kFftPiece / 256;
 
 // cos and sin of k pi / 8, k < 8 (the 16th roots of unity)
 __host__ __device__ constexpr double cos16(int k) {
@@ -130,8 +141,8 @@ __device__ __forceinline__ void reg_fft(double2 (&v)[R], double dir) {
 // One in-place Stockham pass of radix R over n points (Ns = product of the earlier
 // radices): every thread loads its R inputs (stride n/R), twiddles them by
 // e^{dir 2 pi i (j mod Ns) r / (Ns R)}, runs an R-point DFT in registers and, after a
-// barrier, stores them at (j / Ns) Ns R + (j mod Ns) + r Ns.  n <= 8192 and 512
-// threads: each thread holds at most 16 points.
+// barrier, stores them at (j / Ns) Ns R + (j mod Ns) + r Ns.  n <= kFftPiece = 4096
+// and 256 threads: each thread holds at most 16 points.
 template <int R>
 __device__ __forceinline__ void stockham_pass(double2 *buf, int n, int Ns, double dir,
                                               const double2 *__restrict__ tw) {
@@ -146,7 +157,7 @@ __device__ __forceinline__ void stockham_pass(double2 *buf, int n, int Ns, doubl
 #pragma unroll
             for (int r = 0; r < R; ++r) v[jj][r] = buf[pidx(j + r * nj)];
             if (Ns > 1) {
-                const int step = jm * (kFftMax / (Ns * R));
+                const int step = jm * (kTwLen / (Ns * R));
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
                     double2 w = __ldg(&tw[step * r]);
@@ -178,7 +189,7 @@ __device__ __noinline__ void stockham_pass_call(double2 *buf, int n, int Ns, dou
     stockham_pass<R>(buf, n, Ns, dir, tw);
 }
 
-// In-place FFT of length n (power of two <= kFftMax) on a padded shared-memory buffer,
+// In-place FFT of length n (power of two <= kFftPiece) on a padded shared-memory buffer,
 // natural order in and out.  dir = -1: e^{-2 pi i jk/n}; +1: e^{+2 pi i jk/n}.
 // Passes of radix 16 with one smaller radix for the remaining bits.
 __device__ __forceinline__ void fft_stockham(double2 *buf, int n, double dir, const double2 *__restrict__ tw) {
@@ -224,24 +235,26 @@ __device__ __forceinline__ double2 fold_synth(const double2 *__restrict__ Fp, co
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, 1) ring_synth_kernel(const int *__restrict__ ring_list,
+__global__ void __launch_bounds__(kFftThreads, 2) ring_synth_kernel(const int *__restrict__ ring_list,
                                                                      const RingDesc *__restrict__ rings, int lmax,
-                                                                  int M, int nrings, long long npix,
-                                                                  const double2 *__restrict__ F_all,
-                                                                  double *__restrict__ maps_all,
-                                                                  const double2 *__restrict__ tw,
-                                                                  const double2 *__restrict__ bh) {
+                                                                     int M, int nrings, long long npix,
+                                                                     const double2 *__restrict__ F_all,
+                                                                     double *__restrict__ maps_all,
+                                                                     double2 *__restrict__ A_all,
+                                                                     double2 *__restrict__ Y_all,
+                                                                     const double2 *__restrict__ tw,
+                                                                     const double2 *__restrict__ bh) {
     extern __shared__ double2 buf[];
     const int r = ring_list ? ring_list[blockIdx.x] : (int)blockIdx.x;
     const RingDesc rd = rings[r];
-    const int N = rd.N;
+    const int N = rd.N, Q = rd.Q;
     const bool shifted = rd.phi0 != 0.0;
     constexpr int nchan = SPIN ? 2 : 1;
     const double2 *Fp = F_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     const double2 *Fm = SPIN ? Fp + (size_t)nrings * M : Fp;
     double *outQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     double *outU = outQ + npix;
-    if (rd.mode == kDirect) {
+    if (rd.mode == kDirect && Q == 1) {
         for (int k = threadIdx.x; k < N; k += blockDim.x) {
             const double2 d = fold_synth(Fp, Fm, k, N, lmax, shifted);
             buf[pidx(k)] = shifted ? cmul(d, cis_pi(k, N, 0, 1)) : d;
@@ -255,32 +268,56 @@ __global__ void __launch_bounds__(kFftThreads, 1) ring_synth_kernel(const int *_
         }
         return;
     }
-    const int P = rd.P, Q = rd.Q, Pp = P / Q;
+    // Transform of length L (N, or the chirp-z length P) in Q pieces of Lp points.  One
+    // pass writes the phased (and chirped) fold a[k] to the ring's scratch row; piece s
+    // then folds a[k] e^{-+2 pi i s k / L} modulo Lp with table twiddles.
+    const bool blue = rd.mode == kBluestein;
+    const int L = blue ? rd.P : N, Lp = L / Q;
+    double2 *Ag = A_all + (size_t)blockIdx.y * npix + rd.start;
+    double2 *Yg = Y_all + (size_t)blockIdx.y * npix + rd.start;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        const double2 d = fold_synth(Fp, Fm, k, N, lmax, shifted);
+        // e^{i pi k / N} ring phase; chirp-z: times w(k) = e^{i pi k^2 / N}
+        const int ph = (shifted ? k : 0) + (blue ? (k * k) % (2 * N) : 0);
+        Ag[k] = ph ? cmul(d, cis_pi(ph, N, 0, 1)) : d;
+    }
+    __syncthreads();
     const double2 *B = bh + rd.bh_off;
     for (int s = 0; s < Q; ++s) {
-        // piece s of FFT_P(a), a[k] = D[k] w(k): fold a[k] e^{-2 pi i s k / P} modulo Pp
-        for (int q = threadIdx.x; q < Pp; q += blockDim.x) {
+        for (int q = threadIdx.x; q < Lp; q += blockDim.x) {
             double2 v = make_double2(0.0, 0.0);
-            for (int k = q; k < N; k += Pp) {
-                // D[k] w(k) e^{-2 pi i s k / P}, w(k) = e^{i pi k^2 / N}, with the ring phase folded in
-                const int ph = (k * k) % (2 * N) + (shifted ? k : 0);
-                v = cadd(v, cmul(fold_synth(Fp, Fm, k, N, lmax, shifted), cis_pi(ph, N, -s * k, P)));
+            for (int k = q; k < N; k += Lp) {
+                const double2 a = Ag[k];
+                // direct: inverse DFT, e^{+2 pi i s k / N}; chirp-z: FFT_P, e^{-2 pi i s k / P}
+                v = cadd(v, s ? cmul(a, twid(tw, s * k, L, !blue)) : a);
             }
             buf[pidx(q)] = v;
         }
         __syncthreads();
-        fft_stockham(buf, Pp, -1.0, tw);
-        for (int q = threadIdx.x; q < Pp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, P, Q * q + s, 1));
+        if (!blue) {
+            fft_stockham(buf, Lp, +1.0, tw);
+            for (int q = threadIdx.x; q < Lp; q += blockDim.x) {
+                const double2 v = buf[pidx(q)];
+                outQ[Q * q + s] = v.x;
+                if (SPIN) outU[Q * q + s] = v.y;
+            }
+            __syncthreads();
+            continue;
+        }
+        fft_stockham(buf, Lp, -1.0, tw);
+        for (int q = threadIdx.x; q < Lp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, L, Q * q + s, 1));
         __syncthreads();
-        fft_stockham(buf, Pp, +1.0, tw);
+        fft_stockham(buf, Lp, +1.0, tw);
+        // y[j] += conv_s[j mod Lp] e^{2 pi i s j / P}; the chirp is applied once after the last piece
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            const double2 v = cmul(buf[pidx(j & (Pp - 1))], cis_pi((j * j) % (2 * N), N, s * j, P));
-            if (s == 0) {
+            double2 v = buf[pidx(j & (Lp - 1))];
+            if (s) v = cadd(Yg[j], cmul(v, twid(tw, s * j, L, true)));
+            if (s < Q - 1) {
+                Yg[j] = v;
+            } else {
+                v = cmul(v, cis_pi((j * j) % (2 * N), N, 0, 1));
                 outQ[j] = v.x;
                 if (SPIN) outU[j] = v.y;
-            } else {
-                outQ[j] += v.x;
-                if (SPIN) outU[j] += v.y;
             }
         }
         __syncthreads();
@@ -306,50 +343,69 @@ __device__ __forceinline__ void gather_adjoint(const double2 *W, int N, int lmax
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, 1) ring_adjoint_kernel(const int *__restrict__ ring_list,
+__global__ void __launch_bounds__(kFftThreads, 2) ring_adjoint_kernel(const int *__restrict__ ring_list,
                                                                        const RingDesc *__restrict__ rings, int lmax,
-                                                                    int M, int nrings, long long npix,
-                                                                    const double *__restrict__ maps_all,
-                                                                    double2 *__restrict__ V_all,
-                                                                    double2 *__restrict__ W_all,
-                                                                    const double2 *__restrict__ tw,
-                                                                    const double2 *__restrict__ bh) {
+                                                                       int M, int nrings, long long npix,
+                                                                       const double *__restrict__ maps_all,
+                                                                       double2 *__restrict__ V_all,
+                                                                       double2 *__restrict__ A_all,
+                                                                       double2 *__restrict__ W_all,
+                                                                       const double2 *__restrict__ tw,
+                                                                       const double2 *__restrict__ bh) {
     extern __shared__ double2 buf[];
     const int r = ring_list ? ring_list[blockIdx.x] : (int)blockIdx.x;
     const RingDesc rd = rings[r];
-    const int N = rd.N;
+    const int N = rd.N, Q = rd.Q;
     const bool shifted = rd.phi0 != 0.0;
     constexpr int nchan = SPIN ? 2 : 1;
     const double *inQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     const double *inU = inQ + npix;
     double2 *Vp = V_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     double2 *Vm = SPIN ? Vp + (size_t)nrings * M : Vp;
-    if (rd.mode == kDirect) {
+    if (rd.mode == kDirect && Q == 1) {
         for (int j = threadIdx.x; j < N; j += blockDim.x) buf[pidx(j)] = make_double2(inQ[j], SPIN ? inU[j] : 0.0);
         __syncthreads();
         fft_stockham(buf, N, -1.0, tw);
         gather_adjoint<SPIN, true>(buf, N, lmax, shifted, Vp, Vm);
         return;
     }
-    const int P = rd.P, Q = rd.Q, Pp = P / Q;
-    const double2 *B = bh + rd.bh_off;
+    // Forward transform of length L (N, or P) in Q pieces of Lp points; the spectrum
+    // W[k], k < N, is assembled in the ring's scratch row and then gathered.
+    const bool blue = rd.mode == kBluestein;
+    const int L = blue ? rd.P : N, Lp = L / Q;
+    double2 *Ag = A_all + (size_t)blockIdx.y * npix + rd.start;
     double2 *Wg = W_all + (size_t)blockIdx.y * npix + rd.start;
+    if (blue) {  // chirped input a[j] = v[j] conj(w(j)), once
+        for (int j = threadIdx.x; j < N; j += blockDim.x)
+            Ag[j] = cmul(make_double2(inQ[j], SPIN ? inU[j] : 0.0), cis_pi(-((j * j) % (2 * N)), N, 0, 1));
+        __syncthreads();
+    }
+    const double2 *B = bh + rd.bh_off;
     for (int s = 0; s < Q; ++s) {
-        for (int q = threadIdx.x; q < Pp; q += blockDim.x) {
+        for (int q = threadIdx.x; q < Lp; q += blockDim.x) {
             double2 v = make_double2(0.0, 0.0);
-            for (int j = q; j < N; j += Pp)
-                v = cadd(v, cmul(make_double2(inQ[j], SPIN ? inU[j] : 0.0), cis_pi(-((j * j) % (2 * N)), N, -s * j, P)));
+            for (int j = q; j < N; j += Lp) {
+                const double2 a = blue ? Ag[j] : make_double2(inQ[j], SPIN ? inU[j] : 0.0);
+                v = cadd(v, s ? cmul(a, twid(tw, s * j, L, false)) : a);  // e^{-2 pi i s j / L}
+            }
             buf[pidx(q)] = v;
         }
         __syncthreads();
-        fft_stockham(buf, Pp, -1.0, tw);
-        for (int q = threadIdx.x; q < Pp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, P, Q * q + s, -1));
+        fft_stockham(buf, Lp, -1.0, tw);
+        if (!blue) {  // W[Q q + s]
+            for (int q = threadIdx.x; q < Lp; q += blockDim.x) Wg[Q * q + s] = buf[pidx(q)];
+            __syncthreads();
+            continue;
+        }
+        for (int q = threadIdx.x; q < Lp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, L, Q * q + s, -1));
         __syncthreads();
-        fft_stockham(buf, Pp, +1.0, tw);
-        // W[k] = w'(k) conv[k], accumulated over the pieces in the ring's slot of the scratch
+        fft_stockham(buf, Lp, +1.0, tw);
+        // W[k] = conj(w(k)) sum_s conv_s[k mod Lp] e^{2 pi i s k / P}, the chirp after the last piece
         for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            const double2 v = cmul(buf[pidx(k & (Pp - 1))], cis_pi(-((k * k) % (2 * N)), N, s * k, P));
-            Wg[k] = s ? cadd(Wg[k], v) : v;
+            double2 v = buf[pidx(k & (Lp - 1))];
+            if (s) v = cadd(Wg[k], cmul(v, twid(tw, s * k, L, true)));
+            if (s == Q - 1) v = cmul(v, cis_pi(-((k * k) % (2 * N)), N, 0, 1));
+            Wg[k] = v;
         }
         __syncthreads();
     }
@@ -366,7 +422,7 @@ __global__ void __launch_bounds__(kFftThreads) bluestein_setup_kernel(const int 
     const int N = lens[blockIdx.x];
     int P = 1;
     while (P < 2 * N - 1) P <<= 1;
-    const int Q = P > kFftMax ? P / kFftMax : 1;
+    const int Q = P > kFftPiece ? P / kFftPiece : 1;
     const int s = blockIdx.y;
     if (s >= Q) return;
     const int Pp = P / Q;
@@ -411,11 +467,11 @@ int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cud
     if (p.spin == 0) {
         if ((rc = ensure_smem(ring_synth_kernel<0>))) return rc;
         ring_synth_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
-                                                                     maps, p.d_tw, p.d_bh);
+                                                                     maps, p.d_W, p.d_W2, p.d_tw, p.d_bh);
     } else {
         if ((rc = ensure_smem(ring_synth_kernel<2>))) return rc;
         ring_synth_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
-                                                                     maps, p.d_tw, p.d_bh);
+                                                                     maps, p.d_W, p.d_W2, p.d_tw, p.d_bh);
     }
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
@@ -428,11 +484,11 @@ int launch_ring_adjoint(const Plan &p, const double *maps, double2 *V, double2 *
     if (p.spin == 0) {
         if ((rc = ensure_smem(ring_adjoint_kernel<0>))) return rc;
         ring_adjoint_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix,
-                                                                       maps, V, W, p.d_tw, p.d_bh);
+                                                                       maps, V, p.d_W2, W, p.d_tw, p.d_bh);
     } else {
         if ((rc = ensure_smem(ring_adjoint_kernel<2>))) return rc;
         ring_adjoint_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix,
-                                                                       maps, V, W, p.d_tw, p.d_bh);
+                                                                       maps, V, p.d_W2, W, p.d_tw, p.d_bh);
     }
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
@@ -442,7 +498,7 @@ int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *o
     if (nlen <= 0) return JHTB_OK;
     int rc;
     if ((rc = ensure_smem(bluestein_setup_kernel))) return rc;
-    dim3 grid(nlen, 4);
+    dim3 grid(nlen, 8);
     bluestein_setup_kernel<<<grid, kFftThreads, smem_bytes(), s>>>(lengths, offs, p.d_tw, p.d_bh);
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
