@@ -313,3 +313,53 @@ def test_constrained_realization_matches_oracle_with_the_same_sources(spin):
     assert np.all(draw[..., ells < 2] == 0)  # pinned modes are exactly zero in every draw
     mean = _np(jhtb.wiener(maps, cl, nside, lmax, spin, inv_noise=inv_noise, tol=1e-11))
     assert relerr(draw, mean) > 1e-3  # a draw, not the mean
+
+
+
+@pytest.mark.slow
+def test_masked_cg_16_rhs_at_nside512_converges():
+    """Batched masked CG at nside 512, lmax 1024: a |cos theta| < 0.34 cut plus 200 seeded
+    1-degree discs, data S a + white noise (sigma 1e-2), 16 right-hand sides to relative
+    residual 1e-8 with eps = 1e-6 of the largest diagonal entry of T S^T (M W) S T^-1.
+    Every column reaches the tolerance and the returned a_lm satisfies the system."""
+    from jht_b200 import masked as MK
+
+    nside, lmax, spin, B = 512, 1024, 0, 16
+    npix = 12 * nside * nside
+    rng = np.random.default_rng(16)
+    geo = jhtb.healpix.RingInfo(nside)
+    z = np.repeat(geo.z, geo.npix_ring)
+    phi = np.concatenate([geo.phi0[r] + 2 * np.pi * np.arange(n) / n for r, n in enumerate(geo.npix_ring)])
+    st = np.sqrt(1 - z * z)
+    mask = (np.abs(z) >= 0.34).astype(np.float64)
+    cz = rng.uniform(-1, 1, 200)
+    cp = rng.uniform(0, 2 * np.pi, 200)
+    cs = np.sqrt(1 - cz * cz)
+    cos_r = np.cos(np.radians(1.0))
+    for k in range(200):
+        mask[z * cz[k] + st * cs[k] * np.cos(phi - cp[k]) > cos_r] = 0.0
+    ell = np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
+    K = jhtb.alm_size(lmax)
+    cl = 1.0 / (ell + 10.0) ** 2
+    a = np.sqrt(cl / 2) * (rng.standard_normal((B, K)) + 1j * rng.standard_normal((B, K)))
+    a[:, : lmax + 1] = np.sqrt(cl[: lmax + 1]) * rng.standard_normal((B, lmax + 1))
+    gen = torch.Generator("cuda").manual_seed(16)
+    maps = jhtb.synthesis_batch(a, nside, lmax, spin)
+    maps = maps + 1e-2 * torch.randn(maps.shape, dtype=torch.float64, device="cuda", generator=gen)
+    w = MK._weight_pix(nside, npix, maps.device, mask=mask)
+    # diagonal entries on 16 m = 0 columns: m = 0 functions keep the most weight near the
+    # poles, outside the |cos theta| < 0.34 cut, so the largest of them bounds the diagonal
+    probe = torch.zeros((16, MK.n_dof(lmax, spin)), dtype=torch.float64, device="cuda")
+    cols = torch.as_tensor(np.linspace(0, lmax, 16).astype(np.int64), device="cuda")
+    probe[torch.arange(16, device="cuda"), cols] = 1.0
+    diag = MK._normal(probe, w, nside, lmax, spin, "fp64")[torch.arange(16, device="cuda"), cols]
+    eps = 1e-6 * float(diag.max())
+    assert 0.5 < float(diag.max()) <= 1.0 + 1e-6
+    sol, info = jhtb.deconvolve_batch(maps, mask, nside, lmax, spin, tol=1e-8, reg=eps, max_iter=6000,
+                                      return_info=True)
+    assert bool(torch.all(info["rel_residual"] <= 1e-8)), (info["iterations"], info["rel_residual"])
+    x = MK._real_batch(sol.reshape(B, 1, K), lmax, spin)
+    b = MK._real_batch(jhtb.healpix._adjoint_raw(w * maps.reshape(B, 1, npix), nside, lmax, spin, "fp64"), lmax, spin)
+    Ax = MK._normal(x, w, nside, lmax, spin, "fp64") + eps * x
+    rel = torch.linalg.norm(b - Ax, dim=1) / torch.linalg.norm(b, dim=1)
+    assert float(rel.max()) <= 1e-7, float(rel.max())

@@ -48,3 +48,22 @@ def test_bf16x3_synthesis_matches_fp64(nside, lmax, B, spin):
     for b in range(B):
         err = np.max(np.abs(out[b] - ref[b])) / np.max(np.abs(ref[b]))
         assert err <= MIXED_TOL, (b, err)
+
+
+@pytest.mark.slow
+def test_bf16x3_batch64_at_nside512():
+    """64 spin-0 maps at nside 512, lmax 1024, per-map amplitudes log-uniform in [1e-2, 1e2]:
+    every map within 1e-6 of the FP64 synthesis (the batched configuration's error report)."""
+    nside, lmax, B, spin = 512, 1024, 64, 0
+    rng = np.random.default_rng(64)
+    a = _alms(rng, B, lmax, spin, amp_spread=True)
+    a_t = torch.as_tensor(a, device="cuda")
+    out = jhtb.synthesis_batch(a_t, nside, lmax, spin, precision="bf16x3")
+    assert _lib.get_plan(nside, lmax, spin, "bf16x3", B).status() == 0
+    worst = 0.0
+    for b0 in range(0, B, 16):
+        ref = jhtb.synthesis_batch(a_t[b0 : b0 + 16], nside, lmax, spin)
+        got = out[b0 : b0 + 16]
+        err = torch.amax(torch.abs(got - ref), dim=1) / torch.amax(torch.abs(ref), dim=1)
+        worst = max(worst, float(err.max()))
+    assert worst <= MIXED_TOL
