@@ -24,7 +24,7 @@ JHTB_ERR_CUDA = -3
 JHTB_ERR_NOMEM = -4
 
 PRECISIONS = {"fp64": 0, "fp32": 1, "bf16x3": 2}
-TC_MAPS = 8  # maps per tensor-core GEMM group (kTcMaps in the CUDA sources)
+TC_MAPS = 16  # maps per tensor-core GEMM group (kTcMaps in the CUDA sources)
 
 # every exported symbol of include/jhtb.h (checked by the CPU test suite)
 EXPORTS = (
@@ -263,7 +263,7 @@ def get_plan(nside: int, lmax: int, spin: int, precision: str = "fp64", batch: i
         # the tensor-core path shares one recursion among the maps of a pass: hold whole
         # groups of TC_MAPS maps when device memory allows
         free, _ = torch.cuda.mem_get_info(dev)
-        cap = max(1, min(64, min(32 << 30, free // 3) // per))
+        cap = max(1, min(64, min(64 << 30, free // 2) // per))
         if cap >= TC_MAPS:
             cap -= cap % TC_MAPS
     else:

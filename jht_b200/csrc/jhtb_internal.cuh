@@ -44,7 +44,20 @@ constexpr double kLn2x400 = 277.25887222397812;       // 400 ln 2
 #endif
 constexpr int kR0 = JHTB_R0;  // spin 0
 constexpr int kR2 = JHTB_R2;  // spin 2
-constexpr int kTcMaps = 8;    // maps per tensor-core pass (N = 4 * maps per GEMM)
+// The adjoint sums each l over the rings of a warp tile: wider tiles (more rings per
+// lane) spend fewer instructions on the cross-lane sum per ring.
+#ifndef JHTB_RA0
+#define JHTB_RA0 4
+#endif
+#ifndef JHTB_RA2
+#define JHTB_RA2 4
+#endif
+constexpr int kRA0 = JHTB_RA0;  // adjoint, spin 0
+constexpr int kRA2 = JHTB_RA2;  // adjoint, spin 2
+#ifndef JHTB_TC_MAPS
+#define JHTB_TC_MAPS 8
+#endif
+constexpr int kTcMaps = JHTB_TC_MAPS;  // maps per tensor-core pass (N = 4 * maps per GEMM)
 
 // FFT: largest power-of-two length handled in one CTA's shared memory.
 constexpr int kFftMax = 8192;    // largest power-of-two ring handled by the direct path per piece plan
@@ -105,18 +118,25 @@ struct Plan {
 
     // Legendre work items (plan creation): start l and recursion state per (m, warp tile),
     // cost-sorted item orders for the persistent kernels
-    int ntiles;          // warp tiles per m
-    int nsuper, tps;     // adjoint: ring quarters per m, warp tiles per quarter
+    int ntiles;          // synthesis warp tiles per m (32 kR rings)
     int *d_lw;           // [M * ntiles]
     double2 *d_st;       // [M * ntiles][nrec][R][32]
     int *d_stsc;         // [M * ntiles][nrec][R][32]
     int *d_synth_order;  // [M * ntiles]
+    // adjoint warp tiles (32 kRA rings): the synthesis tables when kRA == kR
+    int a_ntiles;
+    int nsuper, tps;     // ring quarters per m, adjoint warp tiles per quarter
+    int *d_a_lw;
+    double2 *d_a_st;
+    int *d_a_stsc;
+    bool a_owns_tables;
     int *d_adj_order;    // [M * nsuper]
     int *d_adj_tiles;    // [M * nsuper][tps]
     unsigned *d_counter; // work-queue counter
     double2 *d_part;     // [chunk][nsuper][ncomp][K] adjoint partial sums
 
-    // tensor-core path (precision BF16X3): 128-ring tiles (start tables built with R = 4)
+    // tensor-core path (precision BF16X3): 128-ring (spin 2) or 256-ring (spin 0) tiles;
+    // the start tables are the adjoint's when their tile widths agree
     int tc_ntiles;
     int *d_tc_lw;
     double2 *d_tc_st;
@@ -132,7 +152,7 @@ struct Plan {
     int tc_norder;        // entries of d_tc_order
     int *d_ring_list;     // [nring_list] ring indices of the range, or null for all rings
     int nring_list;
-    std::vector<int> h_lw, h_tc_lw;  // start l per item, kept for re-sorting
+    std::vector<int> h_lw, h_a_lw, h_tc_lw;  // start l per item, kept for re-sorting
 
     // workspace
     double2 *d_F;       // [chunk][nchan][nrings][M] ring spectra

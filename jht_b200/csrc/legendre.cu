@@ -493,40 +493,40 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth2_kernel(LegParams p
 // =====================================================================================
 // adjoint
 // =====================================================================================
-// After the call, lane l holds in v[0] the warp total of entry scatter_index(l).
-template <int NV>
-__device__ __forceinline__ void warp_reduce_scatter(double2 (&v)[NV], int lane) {
-    int mask = 16;
-#pragma unroll
-    for (int half = NV / 2; half >= 1; half /= 2, mask >>= 1) {
-        const bool up = lane & mask;
-#pragma unroll
-        for (int i = 0; i < half; ++i) {
-            const double2 send = up ? v[i] : v[i + half];
-            const double2 keep = up ? v[i + half] : v[i];
-            const double rx = __shfl_xor_sync(kFull, send.x, mask);
-            const double ry = __shfl_xor_sync(kFull, send.y, mask);
-            v[i] = make_double2(keep.x + rx, keep.y + ry);
-        }
-    }
-    for (; mask >= 1; mask >>= 1) {
-        v[0].x += __shfl_xor_sync(kFull, v[0].x, mask);
-        v[0].y += __shfl_xor_sync(kFull, v[0].y, mask);
-    }
-}
+// Warp sum of NE per-lane values through shared memory (no shuffles or selects on the
+// step path): every lane stores its NE values (one 16-byte row slot per entry), then
+// LPE = 32 / NE lanes share each entry, each adding 32 / LPE of the rows in a fixed order
+// (two interleaved chains), and a final xor-shuffle combines the LPE partial sums.
+// A row holds 32 + LPE slots: with that padding both the stores (8 consecutive slots per
+// quarter warp) and the loads (8 distinct 16-byte bank groups per quarter warp) are
+// conflict-free.
+template <int NE>
+struct RedBuf {
+    static constexpr int LPE = 32 / NE;
+    double2 v[NE][32 + LPE];
+};
 
-template <int NV>
-__device__ __forceinline__ int scatter_index(int lane) {
-    int idx = 0, bit = NV / 2;
-    for (int mask = 16; bit >= 1; mask >>= 1, bit >>= 1)
-        if (lane & mask) idx += bit;
-    return idx;
-}
-
-template <int NV>
-__device__ __forceinline__ bool scatter_writer(int lane) {
-    constexpr int used = NV == 4 ? 2 : (NV == 8 ? 3 : (NV == 16 ? 4 : 5));
-    return (lane & ((1 << (5 - used)) - 1)) == 0;
+template <int NE>
+__device__ __forceinline__ double2 red_sum(const RedBuf<NE> &rb, int lane) {
+    constexpr int LPE = RedBuf<NE>::LPE;
+    constexpr int NK = 32 / LPE;
+    const int e = lane / LPE, h = lane % LPE;
+    double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < NK; k += 2) {
+        const double2 a = rb.v[e][LPE * k + h], b = rb.v[e][LPE * (k + 1) + h];
+        s0.x += a.x;
+        s0.y += a.y;
+        s1.x += b.x;
+        s1.y += b.y;
+    }
+    double2 s = make_double2(s0.x + s1.x, s0.y + s1.y);
+#pragma unroll
+    for (int msk = 1; msk < LPE; msk <<= 1) {
+        s.x += __shfl_xor_sync(kFull, s.x, msk);
+        s.y += __shfl_xor_sync(kFull, s.y, msk);
+    }
+    return s;
 }
 
 struct AStage {
@@ -556,8 +556,11 @@ template <int R>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj0_kernel(LegParams p, const double2 *__restrict__ V_all,
                                                                    double2 *__restrict__ part_all, int nb) {
     __shared__ AStage stage[kWarpsPerBlock];
+    __shared__ RedBuf<kSub> red[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     AStage &sb = stage[threadIdx.x >> 5];
+    RedBuf<kSub> &rb = red[threadIdx.x >> 5];
+    constexpr int LPE = RedBuf<kSub>::LPE;
     const int nsup = p.M * p.nsuper;
     const int L = p.lmax;
     for (;;) {
@@ -606,32 +609,31 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj0_kernel(LegParams p, 
                 if (lane < cnt) sb.ag[lane].x = p.alpha[b0 + i0 + lane];
                 __syncwarp();
                 for (int q0 = 0; q0 < cnt; q0 += kSub) {
-                    double2 v[kSub];
                     // the writer lane's output slot is known up front: issue its load of
                     // the running row sum now so the L2 round trip overlaps the steps
-                    const int qw = q0 + scatter_index<kSub>(lane);
-                    const bool wr = scatter_writer<kSub>(lane) && qw < cnt;
+                    const int qw = q0 + lane / LPE;
+                    const bool wr = (lane % LPE) == 0 && qw < cnt;
                     double2 prev = make_double2(0.0, 0.0);
                     if (acc && wr) prev = part[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
 #pragma unroll
                     for (int q = 0; q < kSub; q += 2) {
                         if (q0 + q < cnt)
-                            v[q] = f ? adj0_step<R, false>(sb.ag[q0 + q].x, x, u1, u2, sc, UA)
-                                     : adj0_step<R, true>(sb.ag[q0 + q].x, x, u1, u2, sc, UA);
-                        else v[q] = make_double2(0.0, 0.0);
+                            rb.v[q][lane] = f ? adj0_step<R, false>(sb.ag[q0 + q].x, x, u1, u2, sc, UA)
+                                              : adj0_step<R, true>(sb.ag[q0 + q].x, x, u1, u2, sc, UA);
                         if (q0 + q + 1 < cnt)
-                            v[q + 1] = f ? adj0_step<R, false>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB)
-                                         : adj0_step<R, true>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB);
-                        else v[q + 1] = make_double2(0.0, 0.0);
+                            rb.v[q + 1][lane] = f ? adj0_step<R, false>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB)
+                                                  : adj0_step<R, true>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB);
                     }
                     if (!f) {
                         fast = true;
 #pragma unroll
                         for (int r = 0; r < R; ++r) fast &= sc[r] == 0;
                     }
-                    warp_reduce_scatter<kSub>(v, lane);
-                    if (wr) part[b0 + i0 + qw] = make_double2(v[0].x + prev.x, v[0].y + prev.y);
+                    __syncwarp();
+                    const double2 tot = red_sum<kSub>(rb, lane);
+                    __syncwarp();
+                    if (wr) part[b0 + i0 + qw] = make_double2(tot.x + prev.x, tot.y + prev.y);
                 }
                 __syncwarp();
             }
@@ -690,8 +692,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj2_kernel(LegParams p, 
                                                                    double2 *__restrict__ part_all, int nb) {
     constexpr int NV = 2 * kSub;
     __shared__ AStage stage[kWarpsPerBlock];
+    __shared__ RedBuf<NV> red[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     AStage &sb = stage[threadIdx.x >> 5];
+    RedBuf<NV> &rb = red[threadIdx.x >> 5];
+    constexpr int LPE = RedBuf<NV>::LPE;
     const int nsup = p.M * p.nsuper;
     const int L = p.lmax;
     for (;;) {
@@ -752,27 +757,27 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj2_kernel(LegParams p, 
                 if (lane < cnt) sb.ag[lane] = make_double2(p.alpha[b0 + i0 + lane], p.gamma[b0 + i0 + lane]);
                 __syncwarp();
                 for (int q0 = 0; q0 < cnt; q0 += kSub) {
-                    double2 v[NV];
-                    const int e = scatter_index<NV>(lane);  // 0..kSub-1: p2, kSub..: m2
+                    const int e = lane / LPE;  // entry of this lane's sum: 0..kSub-1 p2, kSub.. m2
                     const int qw = q0 + (e & (kSub - 1));
-                    const bool wr = scatter_writer<NV>(lane) && qw < cnt;
+                    const bool wr = (lane % LPE) == 0 && qw < cnt;
                     double2 *dstw = e >= kSub ? partM : partP;
                     double2 prev = make_double2(0.0, 0.0);
                     if (acc && wr) prev = dstw[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
 #pragma unroll
                     for (int q = 0; q < kSub; q += 2) {
+                        double2 op, om;
                         if (q0 + q < cnt) {
-                            if (f) adj2_step<R, false, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
-                            else adj2_step<R, true, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, v[q], v[kSub + q]);
-                        } else {
-                            v[q] = v[kSub + q] = make_double2(0.0, 0.0);
+                            if (f) adj2_step<R, false, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                            else adj2_step<R, true, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                            rb.v[q][lane] = op;
+                            rb.v[kSub + q][lane] = om;
                         }
                         if (q0 + q + 1 < cnt) {
-                            if (f) adj2_step<R, false, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
-                            else adj2_step<R, true, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, v[q + 1], v[kSub + q + 1]);
-                        } else {
-                            v[q + 1] = v[kSub + q + 1] = make_double2(0.0, 0.0);
+                            if (f) adj2_step<R, false, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                            else adj2_step<R, true, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                            rb.v[q + 1][lane] = op;
+                            rb.v[kSub + q + 1][lane] = om;
                         }
                     }
                     if (!f) {
@@ -780,8 +785,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) adj2_kernel(LegParams p, 
 #pragma unroll
                         for (int r = 0; r < R; ++r) fast &= (sp[r] == 0) && (sm[r] == 0);
                     }
-                    warp_reduce_scatter<NV>(v, lane);
-                    if (wr) dstw[b0 + i0 + qw] = make_double2(v[0].x + prev.x, v[0].y + prev.y);
+                    __syncwarp();
+                    const double2 tot = red_sum<NV>(rb, lane);
+                    __syncwarp();
+                    if (wr) dstw[b0 + i0 + qw] = make_double2(tot.x + prev.x, tot.y + prev.y);
                 }
                 __syncwarp();
             }
@@ -903,11 +910,15 @@ int launch_legendre_adjoint(const Plan &p, const double2 *F, double2 *alm, int n
     if (nb <= 0) return JHTB_OK;
     JHTB_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned), s));
     LegParams q = make_params(p);
+    q.ntiles = p.a_ntiles;
+    q.lw = p.d_a_lw;
+    q.st = p.d_a_st;
+    q.stsc = p.d_a_stsc;
     if (p.spin == 0) {
-        auto k = adj0_kernel<kR0>;
+        auto k = adj0_kernel<kRA0>;
         k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
     } else {
-        auto k = adj2_kernel<kR2>;
+        auto k = adj2_kernel<kRA2>;
         k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
     }
     JHTB_CUDA_TRY(cudaGetLastError());

@@ -89,11 +89,17 @@ void free_plan(Plan *p) {
                     p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err, p->d_ring_list};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    if (p->a_owns_tables) {
+        void *a[] = {p->d_a_lw, p->d_a_st, p->d_a_stsc};
+        for (void *q : a)
+            if (q) cudaFree(q);
+    }
     if (p->tc_owns_tables) {
-        void *tc[] = {p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, p->d_tc_order};
+        void *tc[] = {p->d_tc_lw, p->d_tc_st, p->d_tc_stsc};
         for (void *q : tc)
             if (q) cudaFree(q);
     }
+    if (p->d_tc_order) cudaFree(p->d_tc_order);
     for (auto &e : p->events) {
         cudaEventDestroy(e.start);
         cudaEventDestroy(e.stop);
@@ -114,37 +120,46 @@ int build_orders(Plan *p) {
         return upload(dptr, h, bytes);
     };
     int rc;
-    // FP64 kernels: tiles of 32 R rings
+    // FP64 synthesis: tiles of 32 kR rings, one item each
     {
         const int tw = 32 * (p->spin ? kR2 : kR0);
         const std::vector<int> &lw = p->h_lw;
-        auto in_range = [&](int tile) { return tile * tw >= t0 && tile * tw < t1; };
         auto cost = [&](long long it) { return std::max(0, L + 1 - lw[it]); };
         std::vector<int> so;
-        for (long long i = 0; i < (long long)M * p->ntiles; ++i)
-            if (in_range((int)(i % p->ntiles))) so.push_back((int)i);
+        for (long long i = 0; i < (long long)M * p->ntiles; ++i) {
+            const int tile = (int)(i % p->ntiles);
+            if (tile * tw >= t0 && tile * tw < t1) so.push_back((int)i);
+        }
         std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return cost(a) > cost(b); });
+        p->nsynth = (int)so.size();
+        if ((rc = refresh(&p->d_synth_order, so))) return rc;
+    }
+    // FP64 adjoint: tiles of 32 kRA rings grouped into ring quarters (one item each)
+    {
+        const int tw = 32 * (p->spin ? kRA2 : kRA0);
+        const int nt = p->a_ntiles;
+        const std::vector<int> &lw = p->h_a_lw;
+        auto in_range = [&](int tile) { return tile * tw >= t0 && tile * tw < t1; };
+        auto cost = [&](long long it) { return std::max(0, L + 1 - lw[it]); };
         const long long nsup = (long long)M * p->nsuper;
         std::vector<int> at((size_t)nsup * p->tps, -1), ao(nsup);
         std::vector<long long> acost(nsup, 0);
         for (int m = 0; m < M; ++m)
             for (int s = 0; s < p->nsuper; ++s) {
                 std::vector<int> tl;
-                for (int t = s * p->tps; t < std::min((s + 1) * p->tps, p->ntiles); ++t)
+                for (int t = s * p->tps; t < std::min((s + 1) * p->tps, nt); ++t)
                     if (in_range(t)) tl.push_back(t);
                 std::stable_sort(tl.begin(), tl.end(), [&](int a, int b) {
-                    return lw[(long long)m * p->ntiles + a] < lw[(long long)m * p->ntiles + b];
+                    return lw[(long long)m * nt + a] < lw[(long long)m * nt + b];
                 });
                 const long long si = (long long)m * p->nsuper + s;
                 for (size_t j = 0; j < tl.size(); ++j) {
                     at[si * p->tps + j] = tl[j];
-                    acost[si] += cost((long long)m * p->ntiles + tl[j]);
+                    acost[si] += cost((long long)m * nt + tl[j]);
                 }
                 ao[si] = (int)si;
             }
         std::stable_sort(ao.begin(), ao.end(), [&](int a, int b) { return acost[a] > acost[b]; });
-        p->nsynth = (int)so.size();
-        if ((rc = refresh(&p->d_synth_order, so))) return rc;
         if ((rc = refresh(&p->d_adj_order, ao))) return rc;
         if ((rc = refresh(&p->d_adj_tiles, at))) return rc;
     }
@@ -294,8 +309,6 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         const int R = spin ? kR2 : kR0;
         const int nrec = spin ? 2 : 1;
         p->ntiles = (T + 32 * R - 1) / (32 * R);
-        p->nsuper = std::min(4, p->ntiles);
-        p->tps = (p->ntiles + p->nsuper - 1) / p->nsuper;
         const long long nitems = (long long)M * p->ntiles;
         const size_t nst_el = (size_t)nitems * nrec * R * 32;
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_lw, sizeof(int) * nitems));
@@ -308,6 +321,33 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         p->h_lw.resize(nitems);
         JHTB_CUDA_TRY(cudaMemcpy(p->h_lw.data(), p->d_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
     }
+    {
+        // adjoint tiles of 32 kRA rings (the synthesis tables when the widths agree)
+        const int R = spin ? kR2 : kR0, RA = spin ? kRA2 : kRA0;
+        const int nrec = spin ? 2 : 1;
+        p->a_ntiles = (T + 32 * RA - 1) / (32 * RA);
+        p->nsuper = std::min(4, p->a_ntiles);
+        p->tps = (p->a_ntiles + p->nsuper - 1) / p->nsuper;
+        if (RA == R) {
+            p->a_owns_tables = false;
+            p->d_a_lw = p->d_lw;
+            p->d_a_st = p->d_st;
+            p->d_a_stsc = p->d_stsc;
+            p->h_a_lw = p->h_lw;
+        } else {
+            const long long nitems = (long long)M * p->a_ntiles;
+            const size_t nel = (size_t)nitems * nrec * RA * 32;
+            p->a_owns_tables = true;
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_a_lw, sizeof(int) * nitems));
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_a_st, sizeof(double2) * nel));
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_a_stsc, sizeof(int) * nel));
+            bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nel;
+            if ((rc = launch_start_states_r(*p, RA, p->a_ntiles, p->d_a_lw, p->d_a_st, p->d_a_stsc, 0))) return rc;
+            JHTB_CUDA_TRY(cudaDeviceSynchronize());
+            p->h_a_lw.resize(nitems);
+            JHTB_CUDA_TRY(cudaMemcpy(p->h_a_lw.data(), p->d_a_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
+        }
+    }
 
     // ---- tensor-core path: 128-ring tiles ---------------------------------------------------
     JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_err, sizeof(int)));
@@ -318,17 +358,25 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         const int Rt = spin ? 4 : 8;
         const int nrec = spin ? 2 : 1;
         p->tc_ntiles = (T + 32 * Rt - 1) / (32 * Rt);
-        const long long nitems = (long long)M * p->tc_ntiles;
-        const size_t nel = (size_t)nitems * nrec * Rt * 32;
-        p->tc_owns_tables = true;
-        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_lw, sizeof(int) * nitems));
-        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_st, sizeof(double2) * nel));
-        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_stsc, sizeof(int) * nel));
-        bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nel;
-        if ((rc = launch_start_states_r(*p, Rt, p->tc_ntiles, p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, 0))) return rc;
-        JHTB_CUDA_TRY(cudaDeviceSynchronize());
-        p->h_tc_lw.resize(nitems);
-        JHTB_CUDA_TRY(cudaMemcpy(p->h_tc_lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
+        if (Rt == (spin ? kRA2 : kRA0)) {
+            p->tc_owns_tables = false;
+            p->d_tc_lw = p->d_a_lw;
+            p->d_tc_st = p->d_a_st;
+            p->d_tc_stsc = p->d_a_stsc;
+            p->h_tc_lw = p->h_a_lw;
+        } else {
+            const long long nitems = (long long)M * p->tc_ntiles;
+            const size_t nel = (size_t)nitems * nrec * Rt * 32;
+            p->tc_owns_tables = true;
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_lw, sizeof(int) * nitems));
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_st, sizeof(double2) * nel));
+            JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tc_stsc, sizeof(int) * nel));
+            bytes += sizeof(int) * nitems + (sizeof(double2) + sizeof(int)) * nel;
+            if ((rc = launch_start_states_r(*p, Rt, p->tc_ntiles, p->d_tc_lw, p->d_tc_st, p->d_tc_stsc, 0))) return rc;
+            JHTB_CUDA_TRY(cudaDeviceSynchronize());
+            p->h_tc_lw.resize(nitems);
+            JHTB_CUDA_TRY(cudaMemcpy(p->h_tc_lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
+        }
     }
     p->ring_t0 = 0;
     p->ring_t1 = T;

@@ -205,8 +205,9 @@ struct TcCfg {
     static constexpr int NG = 2;                    // GEMMs per chunk = recursion chains per producer thread
     static constexpr int NBT = SPIN ? 2 : 1;        // B tiles per chunk (spin 0: both GEMMs share one)
     static constexpr int N = 4 * BM;                // columns per GEMM
-    static constexpr int NPW = 4;                   // producer warps: one thread per A row (TMEM lane)
-    static constexpr int NBW = 4;                   // builder warps: one thread per (l, map) of a chunk
+    static constexpr int CH = BM >= 16 ? 1 : 2;     // recursion chains (GEMMs) per producer thread
+    static constexpr int NPW = 4 * NG / CH;         // producer warps: one thread per A row (TMEM lane) and chain
+    static constexpr int NBW = kTcK * BM / 32;      // builder warps: one thread per (l, map) of a chunk
     static constexpr int MMA_WARP = NPW + NBW;
     static constexpr int NTHREADS = (NPW + NBW + 1) * 32;
     static constexpr int NSA = 2;                   // A stages (in tensor memory)
@@ -216,9 +217,11 @@ struct TcCfg {
     // tensor memory: per GEMM hh and corr block sums, then the A stages
     static constexpr int COL_A = NG * 2 * N;
     static constexpr int NCOL = COL_A + NSA * NG * 3 * ACOLS;
-    static constexpr uint32_t TCOLS = NCOL <= 32 ? 32 : (NCOL <= 64 ? 64 : (NCOL <= 128 ? 128 : 256));
+    static constexpr uint32_t TCOLS =
+        NCOL <= 32 ? 32 : (NCOL <= 64 ? 64 : (NCOL <= 128 ? 128 : (NCOL <= 256 ? 256 : 512)));
+    static constexpr int MIN_CTAS = TCOLS <= 256 ? 2 : 1;  // resident CTAs per SM the tensor memory allows
     static_assert(NBW * 32 == kTcK * BM, "one builder thread per (l, map) of a chunk");
-    static_assert(NCOL <= 256, "tensor memory of two resident CTAs");
+    static_assert(NCOL <= 512, "tensor memory of one SM");
 };
 
 template <int SPIN, int BM>
@@ -281,44 +284,45 @@ __device__ __forceinline__ double tc_step(double t, double &u1, double &u2, int 
     return (SLOW && sc != 0) ? 0.0 : u;
 }
 
-// 16 steps of this thread's two recursion chains, split into BF16 parts and stored as
-// its row (= its tensor-memory lane) of the two GEMMs' three A operands: tA0 / tA1 are
-// the lane-offset tensor-memory addresses of the chains' split-0 operands, the splits
-// following at ACOLS columns apart.  Spin 2: chain 0 is the +2 recursion (+gamma),
-// chain 1 the -2 one (-gamma), same ring; spin 0: the chains are rings row and
+// 16 steps of this thread's CH recursion chains (GEMMs J0 .. J0 + CH - 1), split into
+// BF16 parts and stored as its row (= its tensor-memory lane) of those GEMMs' three A
+// operands: tA[c] is the lane-offset tensor-memory address of chain c's split-0 operand,
+// the splits following at ACOLS columns apart.  Spin 2: GEMM 0 is the +2 recursion
+// (+gamma), GEMM 1 the -2 one (-gamma), same ring; spin 0: the GEMMs are rings row and
 // 128 + row of the item tile (gamma = 0).  Past the end of the column the
 // coefficients are zero, which keeps the state bounded (u_k = -u_{k-2}) while the B
 // rows there are zero; rows past the last ring start from a zero state and stay zero.
 // Each half-chunk first loads its eight coefficient pairs and forms the multipliers
 // t = alpha x +- gamma, so only one FMA per step stays on the dependency chain.
-template <bool SLOW>
-__device__ __forceinline__ void tc_chunk2(const double2 *coef, double x0, double x1, double (&u1)[2], double (&u2)[2],
-                                          int (&sc)[2], uint32_t tA0, uint32_t tA1) {
+template <bool SLOW, int CH, int J0>
+__device__ __forceinline__ void tc_chunk(const double2 *coef, const double (&x)[CH], double (&u1)[CH],
+                                         double (&u2)[CH], int (&sc)[CH], const uint32_t (&tA)[CH]) {
     constexpr uint32_t AC = kTcK / 2;
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
-        double t0[8], t1[8];
+        double t[CH][8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const double2 a = coef[half * 8 + k];
-            t0[k] = fma(a.x, x0, a.y);
-            t1[k] = fma(a.x, x1, -a.y);
+#pragma unroll
+            for (int c = 0; c < CH; ++c) t[c][k] = ((J0 + c) & 1) ? fma(a.x, x[c], -a.y) : fma(a.x, x[c], a.y);
         }
-        uint32_t pk[2][3][4];
+        uint32_t pk[CH][3][4];
 #pragma unroll
         for (int q = 0; q < 8; q += 2) {
-            const double v00 = tc_step<SLOW>(t0[q], u1[0], u2[0], sc[0]);
-            const double v10 = tc_step<SLOW>(t1[q], u1[1], u2[1], sc[1]);
-            const double v01 = tc_step<SLOW>(t0[q + 1], u1[0], u2[0], sc[0]);
-            const double v11 = tc_step<SLOW>(t1[q + 1], u1[1], u2[1], sc[1]);
-            split3_pair(v00, v01, pk[0][0][q / 2], pk[0][1][q / 2], pk[0][2][q / 2]);
-            split3_pair(v10, v11, pk[1][0][q / 2], pk[1][1][q / 2], pk[1][2][q / 2]);
+            double v0[CH], v1[CH];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) v0[c] = tc_step<SLOW>(t[c][q], u1[c], u2[c], sc[c]);
+#pragma unroll
+            for (int c = 0; c < CH; ++c) v1[c] = tc_step<SLOW>(t[c][q + 1], u1[c], u2[c], sc[c]);
+#pragma unroll
+            for (int c = 0; c < CH; ++c) split3_pair(v0[c], v1[c], pk[c][0][q / 2], pk[c][1][q / 2], pk[c][2][q / 2]);
         }
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
+        for (int c = 0; c < CH; ++c)
 #pragma unroll
             for (int sp = 0; sp < 3; ++sp)
-                tmem_st4((j ? tA1 : tA0) + sp * AC + half * 4, pk[j][sp][0], pk[j][sp][1], pk[j][sp][2], pk[j][sp][3]);
+                tmem_st4(tA[c] + sp * AC + half * 4, pk[c][sp][0], pk[c][sp][1], pk[c][sp][2], pk[c][sp][3]);
     }
 }
 
@@ -360,15 +364,17 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
                             uint32_t tbase, int warp, int lane) {
     using C = TcCfg<SPIN, BM>;
     constexpr int N = C::N;
-    const int row = warp * 32 + lane;  // A row = TMEM lane
-    const uint32_t tl = tbase + ((uint32_t)(warp * 32) << 16);
+    constexpr int CH = C::CH;
+    const int row = (warp & 3) * 32 + lane;  // A row = TMEM lane (warp w reaches lanes 32 (w % 4) ..)
+    const int j0 = (warp >> 2) * CH;         // this thread's first GEMM
+    const uint32_t tl = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     float(&acc)[2][C::NG][N][kTcRows] = sm.acc;
     const int nitems = p.norder;
     const int total = nitems * ((nb + BM - 1) / BM);
     const int stride = gridDim.x;
     unsigned gc = 0, bk = 0;
     bool ok = true;
-    // chain j's ring (spin 0: two 128-ring halves of the item tile) and start-state slot
+    // GEMM j's ring (spin 0: two 128-ring halves of the item tile) and start-state slot
     auto ring_of = [&](int tile, int j) { return SPIN ? tile * kTcRows + row : tile * 2 * kTcRows + j * kTcRows + row; };
     auto st_of = [&](int id, int j) { return ((size_t)id * 2 + j) * kTcRows + row; };
     // the next item's id, lmin, lw and start states are loaded one item ahead, the
@@ -377,46 +383,61 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
     int id = tc_order(p, it, nitems, total);
     int id_next = tc_order(p, it + stride, nitems, total);
     int lmin = __ldg(&p.seed[id / p.ntiles].lmin), lwv = __ldg(&p.lw[id]);
-    double2 st[2];
-    int stsc[2];
+    double2 st[CH];
+    int stsc[CH];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-        st[j] = p.st[st_of(id, j)];
-        stsc[j] = p.stsc[st_of(id, j)];
+    for (int c = 0; c < CH; ++c) {
+        st[c] = p.st[st_of(id, j0 + c)];
+        stsc[c] = p.stsc[st_of(id, j0 + c)];
     }
     for (; it < total && ok; it += stride) {
         if (tc_failed(&sm.fail)) break;
         const int id_nn = tc_order(p, it + 2 * stride, nitems, total);
         const int lmin_n = __ldg(&p.seed[id_next / p.ntiles].lmin), lw_n = __ldg(&p.lw[id_next]);
-        double2 st_n[2];
-        int stsc_n[2];
+        double2 st_n[CH];
+        int stsc_n[CH];
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            st_n[j] = p.st[st_of(id_next, j)];
-            stsc_n[j] = p.stsc[st_of(id_next, j)];
+        for (int c = 0; c < CH; ++c) {
+            st_n[c] = p.st[st_of(id_next, j0 + c)];
+            stsc_n[c] = p.stsc[st_of(id_next, j0 + c)];
         }
 
         const int m = id / p.ntiles, tile = id - m * p.ntiles;
-        const int t0 = ring_of(tile, 0), t1 = ring_of(tile, 1);
-        const double x0 = t0 < p.T ? __ldg(&p.x[t0]) : 0.0;
-        const double x1 = SPIN ? x0 : (t1 < p.T ? __ldg(&p.x[t1]) : 0.0);
+        int tr[CH];
+        double x[CH], u1[CH], u2[CH];
+        int sc[CH];
+        bool fast = true;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            tr[c] = ring_of(tile, j0 + c);
+            x[c] = tr[c] < p.T ? __ldg(&p.x[tr[c]]) : 0.0;
+            u1[c] = st[c].x;
+            u2[c] = st[c].y;
+            sc[c] = tr[c] < p.T ? stsc[c] : 0;
+            fast &= sc[c] == 0;
+        }
         const int nst = p.lmax - lmin + 1, i_start = lwv - lmin;
         const int nck = i_start < nst ? (nst - i_start + kTcK - 1) / kTcK : 0;
-        double u1[2] = {st[0].x, st[1].x}, u2[2] = {st[0].y, st[1].y};
-        int sc[2] = {t0 < p.T ? stsc[0] : 0, t1 < p.T ? stsc[1] : 0};
-        bool fast = sc[0] == 0 && sc[1] == 0;
         for (int c = 0; c < nck; ++c, ++gc) {
             const int sA = gc % C::NSA, sB = gc % C::NSB;
             if (!mbar_wait(&sm.fullB[sB], (gc / C::NSB) & 1u)) { ok = false; break; }
             if (gc >= (unsigned)C::NSA && !mbar_wait(&sm.emptyA[sA], ((gc / C::NSA) - 1u) & 1u)) { ok = false; break; }
             tc_fence_after();  // the stage's previous MMAs are complete before it is overwritten
-            const uint32_t tA0 = tl + (uint32_t)(C::COL_A + (sA * C::NG) * 3 * C::ACOLS);
-            const uint32_t tA1 = tA0 + 3 * C::ACOLS;
-            if (__all_sync(0xffffffffu, fast)) {
-                tc_chunk2<false>(sm.coef[sB], x0, x1, u1, u2, sc, tA0, tA1);
+            uint32_t tA[CH];
+#pragma unroll
+            for (int q = 0; q < CH; ++q) tA[q] = tl + (uint32_t)(C::COL_A + (sA * C::NG + j0 + q) * 3 * C::ACOLS);
+            const bool f = __all_sync(0xffffffffu, fast);
+            if (j0 == 0) {
+                if (f) tc_chunk<false, CH, 0>(sm.coef[sB], x, u1, u2, sc, tA);
+                else tc_chunk<true, CH, 0>(sm.coef[sB], x, u1, u2, sc, tA);
             } else {
-                tc_chunk2<true>(sm.coef[sB], x0, x1, u1, u2, sc, tA0, tA1);
-                fast = sc[0] == 0 && sc[1] == 0;
+                if (f) tc_chunk<false, CH, 1>(sm.coef[sB], x, u1, u2, sc, tA);
+                else tc_chunk<true, CH, 1>(sm.coef[sB], x, u1, u2, sc, tA);
+            }
+            if (!f) {
+                fast = true;
+#pragma unroll
+                for (int q = 0; q < CH; ++q) fast &= sc[q] == 0;
             }
             tmem_wait_st();
             tc_fence_before();
@@ -432,33 +453,33 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
                 const bool first_block = c < kFlush;
                 const int b_lo = (it / nitems) * BM, b_cnt = min(BM, nb - b_lo);
 #pragma unroll 1
-                for (int piece = 0; piece < 2 * N / 8; ++piece) {
-                    const int j = piece / (N / 8), c0 = (piece % (N / 8)) * 8;
+                for (int piece = 0; piece < CH * N / 8; ++piece) {
+                    const int q = piece / (N / 8), j = j0 + q, c0 = (piece % (N / 8)) * 8;
                     const uint32_t tg = tl + (uint32_t)(j * 2 * N + c0);
                     float hh[8], co[8];
                     tmem_ld8(tg, hh);
                     tmem_ld8(tg + N, co);
                     float hi[8], lo[8];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const float sblk = hh[q] + co[q];
+                    for (int e = 0; e < 8; ++e) {
+                        const float sblk = hh[e] + co[e];
                         if (first_block) {
-                            hi[q] = sblk;
-                            lo[q] = 0.0f;
+                            hi[e] = sblk;
+                            lo[e] = 0.0f;
                         } else {
-                            hi[q] = acc[0][j][c0 + q][row];
-                            lo[q] = acc[1][j][c0 + q][row];
-                            df_add(hi[q], lo[q], sblk);
+                            hi[e] = acc[0][j][c0 + e][row];
+                            lo[e] = acc[1][j][c0 + e][row];
+                            df_add(hi[e], lo[e], sblk);
                         }
                     }
                     if (!last) {
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            acc[0][j][c0 + q][row] = hi[q];
-                            acc[1][j][c0 + q][row] = lo[q];
+                        for (int e = 0; e < 8; ++e) {
+                            acc[0][j][c0 + e][row] = hi[e];
+                            acc[1][j][c0 + e][row] = lo[e];
                         }
                     } else {
-                        const int t = j ? t1 : t0;
+                        const int t = tr[q];
                         if (t < p.T) {
 #pragma unroll
                             for (int jb = 0; jb < 2; ++jb) {
@@ -466,7 +487,7 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
                                 if (bm >= b_cnt) continue;
                                 double v[4];
 #pragma unroll
-                                for (int q = 0; q < 4; ++q) v[q] = (double)hi[4 * jb + q] + (double)lo[4 * jb + q];
+                                for (int e = 0; e < 4; ++e) v[e] = (double)hi[4 * jb + e] + (double)lo[4 * jb + e];
                                 tc_store_F<SPIN>(p, F_all, b_lo + bm, SPIN ? j : 0, t, m, lmin, v);
                             }
                         }
@@ -483,10 +504,10 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
             const int b_lo = (it / nitems) * BM, b_cnt = min(BM, nb - b_lo);
             const double z[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const int t = j ? t1 : t0;
+            for (int q = 0; q < CH; ++q) {
+                const int t = tr[q];
                 if (t < p.T)
-                    for (int bm = 0; bm < b_cnt; ++bm) tc_store_F<SPIN>(p, F_all, b_lo + bm, SPIN ? j : 0, t, m, lmin, z);
+                    for (int bm = 0; bm < b_cnt; ++bm) tc_store_F<SPIN>(p, F_all, b_lo + bm, SPIN ? j0 + q : 0, t, m, lmin, z);
             }
         }
         id = id_next;
@@ -494,9 +515,9 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
         lmin = lmin_n;
         lwv = lw_n;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            st[j] = st_n[j];
-            stsc[j] = stsc_n[j];
+        for (int q = 0; q < CH; ++q) {
+            st[q] = st_n[q];
+            stsc[q] = stsc_n[q];
         }
     }
     if (!ok) tc_fail(&sm.fail, p.err);
@@ -678,7 +699,7 @@ __device__ void tc_mma(const TcParams &p, TcSmem<SPIN, BM> &sm, int nb, uint32_t
 }
 
 template <int SPIN, int BM>
-__global__ void __launch_bounds__(TcCfg<SPIN, BM>::NTHREADS, 2)
+__global__ void __launch_bounds__(TcCfg<SPIN, BM>::NTHREADS, TcCfg<SPIN, BM>::MIN_CTAS)
     tc_synth_kernel(TcParams p, const double2 *__restrict__ alm_all, double2 *__restrict__ F_all, int nb) {
     using C = TcCfg<SPIN, BM>;
     using S = TcSmem<SPIN, BM>;
