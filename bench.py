@@ -55,7 +55,7 @@ def parse_args():
     ap.add_argument("--lmax", type=int, default=4096)
     ap.add_argument("--cpu-sample-m", type=int, default=48, help="orders in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mixed-batch", type=int, default=8, help="maps per step of the mixed-precision form (0: skip)")
+    ap.add_argument("--mixed-batch", type=int, default=16, help="maps per step of the mixed-precision form (0: skip)")
     ap.add_argument("--mixed-steps", type=int, default=3)
     return ap.parse_args()
 

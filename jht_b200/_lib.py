@@ -262,10 +262,16 @@ def get_plan(nside: int, lmax: int, spin: int, precision: str = "fp64", batch: i
     if precision == "bf16x3":
         # the tensor-core path shares one recursion among the maps of a pass: hold whole
         # groups of TC_MAPS maps when device memory allows
+        cached = _plans.get((dev, nside, lmax, spin, precision))
+        if cached is None or cached.max_batch < min(batch, 64):
+            torch.cuda.empty_cache()  # a new plan: return torch's idle cached blocks first
         free, _ = torch.cuda.mem_get_info(dev)
-        cap = max(1, min(64, min(64 << 30, free // 2) // per))
-        if cap >= TC_MAPS:
-            cap -= cap % TC_MAPS
+        budget = min(64 << 30, max(free // 2, free - (24 << 30)))
+        cap = max(1, min(64, budget // per))
+        for g in (TC_MAPS, 8):
+            if cap >= g:
+                cap -= cap % g
+                break
     else:
         cap = max(1, min(64, (4 << 30) // per))
     want = max(1, min(batch, cap))

@@ -55,7 +55,7 @@ constexpr int kR2 = JHTB_R2;  // spin 2
 constexpr int kRA0 = JHTB_RA0;  // adjoint, spin 0
 constexpr int kRA2 = JHTB_RA2;  // adjoint, spin 2
 #ifndef JHTB_TC_MAPS
-#define JHTB_TC_MAPS 8
+#define JHTB_TC_MAPS 16
 #endif
 constexpr int kTcMaps = JHTB_TC_MAPS;  // maps per tensor-core pass (N = 4 * maps per GEMM)
 

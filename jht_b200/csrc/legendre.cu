@@ -47,6 +47,15 @@ constexpr int kStage = 32;  // steps staged per warp per round (one per lane)
 #define JHTB_ADJ_SUB 8
 #endif
 constexpr int kSub = JHTB_ADJ_SUB;  // adjoint steps per warp reduction
+// resident CTAs per SM the adjoint kernels are compiled for (their register budget)
+#ifndef JHTB_ADJ0_MINB
+#define JHTB_ADJ0_MINB 4
+#endif
+#ifndef JHTB_ADJ2_MINB
+#define JHTB_ADJ2_MINB 3
+#endif
+constexpr int kAdj0MinBlocks = JHTB_ADJ0_MINB;
+constexpr int kAdj2MinBlocks = JHTB_ADJ2_MINB;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct LegParams {
@@ -553,7 +562,7 @@ __device__ __forceinline__ double2 adj0_step(double al, const double (&x)[R], do
 }
 
 template <int R>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) adj0_kernel(LegParams p, const double2 *__restrict__ V_all,
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj0MinBlocks) adj0_kernel(LegParams p, const double2 *__restrict__ V_all,
                                                                    double2 *__restrict__ part_all, int nb) {
     __shared__ AStage stage[kWarpsPerBlock];
     __shared__ RedBuf<kSub> red[kWarpsPerBlock];
@@ -688,7 +697,7 @@ __device__ __forceinline__ void adj2_step(double al, double ga, const double (&x
 }
 
 template <int R>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) adj2_kernel(LegParams p, const double2 *__restrict__ V_all,
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj2MinBlocks) adj2_kernel(LegParams p, const double2 *__restrict__ V_all,
                                                                    double2 *__restrict__ part_all, int nb) {
     constexpr int NV = 2 * kSub;
     __shared__ AStage stage[kWarpsPerBlock];

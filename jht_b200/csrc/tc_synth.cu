@@ -744,15 +744,11 @@ __global__ void __launch_bounds__(TcCfg<SPIN, BM>::NTHREADS, TcCfg<SPIN, BM>::MI
 
 }  // namespace
 
-int tc_smem_bytes(int spin) {
-    return (spin ? (int)sizeof(TcSmem<2, kTcMaps>) : (int)sizeof(TcSmem<0, kTcMaps>)) + 1024;
-}
-
-template <int SPIN>
+template <int SPIN, int BM>
 static int launch_tc_synth_t(const TcParams &q, const double2 *alm, double2 *F, int nb, cudaStream_t s) {
-    using C = TcCfg<SPIN, kTcMaps>;
-    auto k = tc_synth_kernel<SPIN, kTcMaps>;
-    const int smem = tc_smem_bytes(SPIN);
+    using C = TcCfg<SPIN, BM>;
+    auto k = tc_synth_kernel<SPIN, BM>;
+    const int smem = (int)sizeof(TcSmem<SPIN, BM>) + 1024;
     int dev = 0, nsm = 148, smem_sm = 0, regs_sm = 0, resv = 0;
     JHTB_CUDA_TRY(cudaGetDevice(&dev));
     JHTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -794,7 +790,22 @@ int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaS
     q.order = p.d_tc_order;
     q.norder = p.tc_norder;
     q.err = p.d_err;
-    return p.spin ? launch_tc_synth_t<2>(q, alm, F, nb, s) : launch_tc_synth_t<0>(q, alm, F, nb, s);
+    // whole groups of kTcMaps maps share one recursion (one CTA per SM, N = 4 kTcMaps);
+    // a remainder runs in groups of 8 (two CTAs per SM), so a short batch does not pay
+    // for the columns of a full group
+    constexpr int kSmall = 8;
+    const int nbig = kTcMaps > kSmall ? (nb / kTcMaps) * kTcMaps : 0;
+    const int nsmall = nb - nbig;
+    const size_t alm_map = (size_t)p.ncomp * p.K, F_map = (size_t)p.ncomp * p.nrings * p.M;
+    int rc = JHTB_OK;
+    if (nbig > 0)
+        rc = p.spin ? launch_tc_synth_t<2, kTcMaps>(q, alm, F, nbig, s) : launch_tc_synth_t<0, kTcMaps>(q, alm, F, nbig, s);
+    if (rc == JHTB_OK && nsmall > 0) {
+        const double2 *a2 = alm + (size_t)nbig * alm_map;
+        double2 *F2 = F + (size_t)nbig * F_map;
+        rc = p.spin ? launch_tc_synth_t<2, kSmall>(q, a2, F2, nsmall, s) : launch_tc_synth_t<0, kSmall>(q, a2, F2, nsmall, s);
+    }
+    return rc;
 }
 
 }  // namespace jhtb
