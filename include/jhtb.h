@@ -22,6 +22,11 @@
  *   jhtb_weighted_residual  _analysis.py:49-52, :58-60 (W * m and W * (m - S a))
  *   jhtb_axpy               _analysis.py:60  (a + bare_analysis(...)), masked.py:313 (CG updates)
  *   jhtb_dot                masked.py:313  (the inner products of the CG solve)
+ *   jhtb_plan_create_rings  offgrid.py:60-88  (recursion plan at the Clenshaw-Curtis rings)
+ *   jhtb_legendre_synthesis offgrid.py:155-160 (synth_contract at those rings)
+ *   jhtb_legendre_adjoint   offgrid.py:163-168 (adjoint_contract at those rings)
+ *   jhtb_nufft_interp       _nufft.py:164-178 (nufft2d2's window sums)
+ *   jhtb_nufft_spread       _nufft.py:181-188 (nufft2d1's scatter-add)
  */
 #ifndef JHTB_H
 #define JHTB_H
@@ -81,6 +86,16 @@ int jhtb_last_error(char *buf, size_t len);
 int jhtb_plan_create(int nside, int lmax, int spin, int precision, int max_batch,
                      const jhtb_host_tables *tables, jhtb_plan **out);
 
+/* Ring-set plan: the Legendre stage only, on nrings iso-latitude rings symmetric about
+ * the equator (nrings odd; ring t and ring nrings-1-t at cos theta = +-x[t], the middle
+ * ring on the equator).  tables->x (required) holds x[t] >= 0 for the northern rings
+ * t < (nrings + 1) / 2, non-increasing; the other tables fields may be NULL (then
+ * derived from x).  Used for the Clenshaw-Curtis rings of the off-grid transforms
+ * (offgrid.py:60-88: build_recursion_plan at x_cc).  jhtb_synthesis /
+ * jhtb_adjoint_synthesis reject such a plan; use jhtb_legendre_synthesis / _adjoint. */
+int jhtb_plan_create_rings(int nrings, int lmax, int spin, int precision, int max_batch,
+                           const jhtb_host_tables *tables, jhtb_plan **out);
+
 /* Release every device allocation owned by the plan. */
 int jhtb_plan_destroy(jhtb_plan *plan);
 
@@ -99,6 +114,20 @@ int jhtb_synthesis(jhtb_plan *plan, const void *alm, void *maps, int batch, void
  * jhtb_synthesis in the (2 - delta_m0)-weighted alm inner product.
  * healpix.py:390-412. */
 int jhtb_adjoint_synthesis(jhtb_plan *plan, const void *maps, void *alm, int batch, void *stream);
+
+/* The Legendre stage of S alone: alm (device complex128 [batch][ncomp][K]) -> ring
+ * coefficients (device complex128 [batch][ncomp][nrings][lmax+1]),
+ * F[c][r][m] = sum_l lambda^{s_c}_lm(x_r) alm_c[l, m], with the spin-2 channels
+ * -(E + iB) (+2) and -(E - iB) (-2).  offgrid.py:155-160 (synth_contract at the
+ * Clenshaw-Curtis rings); for a HEALPix plan these are healpix.py:280-291's F before
+ * the phase and the ring FFT. */
+int jhtb_legendre_synthesis(jhtb_plan *plan, const void *alm, void *rings, int batch, void *stream);
+
+/* Transpose of jhtb_legendre_synthesis over all rings: rings (complex128
+ * [batch][ncomp][nrings][lmax+1]) -> alm (complex128 [batch][ncomp][K]); spin 0:
+ * a_lm = sum_r lambda_lm(x_r) V[r][m]; spin 2: (1/2)(-p - n), (i/2)(p - n) with p, n the
+ * +2 / -2 channel sums (healpix.py:353-354).  offgrid.py:163-168 (adjoint_contract). */
+int jhtb_legendre_adjoint(jhtb_plan *plan, const void *rings, void *alm, int batch, void *stream);
 
 /* out[i] = w(pix i) * (maps[i] - synth[i]) for every component and map in the
  * batch (synth may be NULL: out = w * maps).  w(pix) = (4 pi / Npix)(1 + ring_w[r'])
@@ -126,6 +155,26 @@ int jhtb_dot(const jhtb_plan *plan, int64_t n, const double *x, const double *y,
  * calls that overlap on the GPU race, so order them on one stream.  The first call
  * on each device looks up the array's address; make it before any stream capture. */
 int jhtb_synthesis_noalloc(int nside, int lmax, const void *alm, void *map, void *stream);
+
+/* ---- 2D NUFFT stages of the off-grid transforms (_nufft.py:150-191) ----
+ * grid: device complex128 [nk][nm] on the (theta, phi) torus; theta, phi: device
+ * float64 [npts]; W: kernel width (6, 8, 10, 14 or 16); beta: the exponential-of-
+ * semicircle shape.  Point (theta, phi) reads or writes the W x W window starting at
+ * ceil(coord n / 2pi - W / 2) on each axis (mod n), weights
+ * exp(beta (sqrt(1 - (2t/W)^2) - 1)).  Any finite or non-finite coordinate stays
+ * inside the grid. */
+
+/* out[j] = sum of the window's weighted cells (complex128 [npts]); with dtheta and
+ * dphi non-NULL also the derivatives of out[j] in theta and phi.  nufft2d2's gather
+ * and window sum (_nufft.py:164-178). */
+int jhtb_nufft_interp(const void *grid, int nk, int nm, int W, double beta, const double *theta,
+                      const double *phi, int64_t npts, void *out, void *dtheta, void *dphi, void *stream);
+
+/* grid += the transpose of jhtb_nufft_interp applied to vals (complex128 [npts]); the
+ * caller zeroes grid first.  FP64 atomic adds: the order of the sums over points is
+ * not fixed.  nufft2d1's scatter-add (_nufft.py:181-188). */
+int jhtb_nufft_spread(const void *vals, const double *theta, const double *phi, int64_t npts, int nk,
+                      int nm, int W, double beta, void *grid, void *stream);
 
 /* ---- sharding over devices (no counterpart in jht, which runs on one device) ----
  * A plan can be restricted to the ring pairs of half-grid rings [t0, t1) (the

@@ -36,6 +36,7 @@ from .masked import (
     wiener,
     wiener_batch,
 )
+from .offgrid import adjoint_synthesis_general, synthesis_general
 from .weights import pixel_weights, ring_weights
 
 __version__ = "0.1.0"
@@ -53,6 +54,8 @@ __all__ = [
     "deconvolve",
     "wiener",
     "constrained_realization",
+    "synthesis_general",
+    "adjoint_synthesis_general",
     "synthesis_real",
     "analysis_real",
     "bandpower",

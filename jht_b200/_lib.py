@@ -45,6 +45,11 @@ EXPORTS = (
     "jhtb_plan_status",
     "jhtb_plan_ring_costs",
     "jhtb_plan_set_ring_range",
+    "jhtb_plan_create_rings",
+    "jhtb_legendre_synthesis",
+    "jhtb_legendre_adjoint",
+    "jhtb_nufft_interp",
+    "jhtb_nufft_spread",
 )
 
 
@@ -100,6 +105,12 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_plan_status": (i32, [vp, ctypes.POINTER(i32)]),
             "jhtb_plan_ring_costs": (i32, [vp, i32, ctypes.POINTER(i64), i32]),
             "jhtb_plan_set_ring_range": (i32, [vp, i32, i32]),
+            "jhtb_plan_create_rings": (i32, [i32, i32, i32, i32, i32, ctypes.POINTER(HostTables),
+                                             ctypes.POINTER(vp)]),
+            "jhtb_legendre_synthesis": (i32, [vp, vp, vp, i32, vp]),
+            "jhtb_legendre_adjoint": (i32, [vp, vp, vp, i32, vp]),
+            "jhtb_nufft_interp": (i32, [vp, i32, i32, i32, ctypes.c_double, dp, dp, i64, vp, vp, vp, vp]),
+            "jhtb_nufft_spread": (i32, [vp, dp, dp, i64, i32, i32, i32, ctypes.c_double, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -145,7 +156,12 @@ def _half_grid_z(nside: int) -> np.ndarray:
 
 
 def host_tables(nside: int, lmax: int, spin: int) -> dict[str, np.ndarray]:
-    x = _half_grid_z(nside)
+    return host_tables_x(_half_grid_z(nside), lmax, spin)
+
+
+def host_tables_x(x: np.ndarray, lmax: int, spin: int) -> dict[str, np.ndarray]:
+    """Seed tables for the northern rings at cos theta = x (poles give log 0 = -inf)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
     with np.errstate(divide="ignore"):
         logsin = np.log(np.sqrt(np.clip(1.0 - x * x, 0.0, 1.0)))
         logch = np.log(np.sqrt(np.clip((1.0 + x) / 2.0, 0.0, 1.0)))
@@ -173,7 +189,9 @@ class Plan:
     """Owns one jhtb plan handle for (nside, lmax, spin, precision) on one device."""
 
     def __init__(self, nside: int, lmax: int, spin: int, precision: str = "fp64", max_batch: int = 1,
-                 device: int | None = None):
+                 device: int | None = None, rings: tuple[int, np.ndarray] | None = None):
+        """``rings = (nrings, x_north)`` makes a ring-set plan (Legendre stage only) instead
+        of a HEALPix plan; ``nside`` is then ignored."""
         import torch
 
         if precision not in PRECISIONS:
@@ -184,17 +202,26 @@ class Plan:
         self.device = torch.cuda.current_device() if device is None else device
         self.ncomp = 1 if spin == 0 else 2
         self.K = (lmax + 1) * (lmax + 2) // 2
-        self.npix = 12 * nside * nside
-        tabs = host_tables(nside, lmax, spin) if spin in (0, 2) else None
+        self.npix = 12 * nside * nside if rings is None else 0
+        self.nrings = 4 * nside - 1 if rings is None else int(rings[0])
+        if rings is None:
+            tabs = host_tables(nside, lmax, spin) if spin in (0, 2) else None
+        else:
+            tabs = host_tables_x(rings[1], lmax, spin) if spin in (0, 2) else {"x": np.ascontiguousarray(rings[1])}
         self._keep = tabs
         ht = None
         if tabs is not None:
-            ht = HostTables(*(tabs[k].ctypes.data for k in ("x", "logsin", "logcos_half", "logsin_half", "seed_logc")))
+            ht = HostTables(*(tabs[k].ctypes.data if k in tabs else None
+                              for k in ("x", "logsin", "logcos_half", "logsin_half", "seed_logc")))
         handle = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            st = self.lib.jhtb_plan_create(nside, lmax, spin, PRECISIONS[precision], max_batch,
-                                           ctypes.byref(ht) if ht is not None else None, ctypes.byref(handle))
-        check(st, "jhtb_plan_create")
+            if rings is None:
+                st = self.lib.jhtb_plan_create(nside, lmax, spin, PRECISIONS[precision], max_batch,
+                                               ctypes.byref(ht) if ht is not None else None, ctypes.byref(handle))
+            else:
+                st = self.lib.jhtb_plan_create_rings(self.nrings, lmax, spin, PRECISIONS[precision], max_batch,
+                                                     ctypes.byref(ht), ctypes.byref(handle))
+        check(st, "jhtb_plan_create" if rings is None else "jhtb_plan_create_rings")
         self.handle = handle
         self._keep = None
 

@@ -97,6 +97,7 @@ struct Plan {
     int M;         // lmax + 1
     long long K;   // packed alm size
     long long npix;
+    bool rings_only;    // ring-set plan (no pixel grid): the Legendre stage only
     int ncomp;     // 1 (spin 0) or 2 (spin 2)
     int npairs;    // m-pairs (m, lmax - m)
 

@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth0_kernel(LegParams p
             if (t < p.T) {
                 F[(size_t)t * p.M + m] = make_double2(Ar[r] + Br[r], Ai[r] + Bi[r]);
                 if (t < p.T - 1)
-                    F[(size_t)(4 * p.nside - 2 - t) * p.M + m] = make_double2(Ar[r] - Br[r], Ai[r] - Bi[r]);
+                    F[(size_t)(p.nrings - 1 - t) * p.M + m] = make_double2(Ar[r] - Br[r], Ai[r] - Bi[r]);
             }
         }
     }
@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth2_kernel(LegParams p
                 Fp[(size_t)t * p.M + m] = make_double2(a.ppr, a.ppi);
                 Fm[(size_t)t * p.M + m] = make_double2(a.mmr, a.mmi);
                 if (t < p.T - 1) {
-                    const size_t rs = (size_t)(4 * p.nside - 2 - t) * p.M + m;
+                    const size_t rs = (size_t)(p.nrings - 1 - t) * p.M + m;
                     Fp[rs] = make_double2(ssign * a.pmr, ssign * a.pmi);
                     Fm[rs] = make_double2(ssign * a.mpr, ssign * a.mpi);
                 }
@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj0MinBlocks) adj0_kern
                 if (t < p.T) {
                     x[r] = p.x[t];
                     vn = V[(size_t)t * p.M + m];
-                    if (t < p.T - 1) vs = V[(size_t)(4 * p.nside - 2 - t) * p.M + m];
+                    if (t < p.T - 1) vs = V[(size_t)(p.nrings - 1 - t) * p.M + m];
                 }
                 // b_l = sum_t lambda (Vn + (-1)^l (-1)^m V_south)  (_recursion.py:472-497)
                 UA[r] = make_double2(vn.x + vs.x, vn.y + vs.y);
@@ -752,7 +752,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj2MinBlocks) adj2_kern
                     d.vpn = Vp[(size_t)t * p.M + m];
                     d.vmn = Vm[(size_t)t * p.M + m];
                     if (t < p.T - 1) {
-                        const size_t rs = (size_t)(4 * p.nside - 2 - t) * p.M + m;
+                        const size_t rs = (size_t)(p.nrings - 1 - t) * p.M + m;
                         const double2 a = Vp[rs], c = Vm[rs];
                         d.spA = make_double2(ssign * a.x, ssign * a.y);
                         d.smA = make_double2(ssign * c.x, ssign * c.y);

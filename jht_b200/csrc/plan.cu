@@ -184,7 +184,7 @@ int build_orders(Plan *p) {
         std::vector<int> rl;
         for (int t = t0; t < t1; ++t) {
             rl.push_back(t);
-            if (t < T - 1) rl.push_back(4 * p->nside - 2 - t);
+            if (t < T - 1) rl.push_back(p->nrings - 1 - t);
         }
         p->nring_list = (int)rl.size();
         if ((rc = upload(&p->d_ring_list, rl, bytes))) return rc;
@@ -201,7 +201,7 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     std::vector<double> z(nr), phi0(nr);
     std::vector<long long> npr(nr), start(nr);
     const double ns2 = 3.0 * (double)((long long)nside * nside);
-    for (int r = 0; r < nr; ++r) {
+    for (int r = 0; r < (p->rings_only ? 0 : nr); ++r) {
         long long i = r + 1;
         if (i < nside) {
             npr[r] = 4 * i;
@@ -382,51 +382,53 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     p->ring_t1 = T;
     if ((rc = build_orders(p))) return rc;
 
-    // ---- ring FFT descriptors -------------------------------------------------------------
-    std::vector<RingDesc> rings(nr);
+    // ---- ring FFT descriptors (HEALPix plans; a ring-set plan stops at the ring spectra) ----
+    std::vector<RingDesc> rings(p->rings_only ? 0 : nr);
     std::map<long long, long long> bh_offset;  // Bluestein length -> offset
     std::vector<int> blens;
     std::vector<long long> boffs;
     long long bh_len = 0;
-    for (int r = 0; r < nr; ++r) {
-        RingDesc &d = rings[r];
-        d.N = (int)npr[r];
-        d.start = start[r];
-        d.phi0 = phi0[r];
-        if (is_pow2(d.N) && d.N <= 8 * kFftPiece) {
-            d.mode = kDirect;
-            d.P = d.N;
-            d.Q = std::max(1, d.N / kFftPiece);
-            d.bh_off = 0;
-        } else {
-            d.mode = kBluestein;
-            d.P = (int)next_pow2(2LL * d.N - 1);
-            d.Q = std::max(1, d.P / kFftPiece);
-            if (d.Q > 8) return fail(JHTB_ERR_UNSUPPORTED, "ring length too large (nside > 4096)");
-            auto it = bh_offset.find(d.N);
-            if (it == bh_offset.end()) {
-                bh_offset[d.N] = bh_len;
-                blens.push_back(d.N);
-                boffs.push_back(bh_len);
-                d.bh_off = bh_len;
-                bh_len += d.P;
+    if (!p->rings_only) {
+        for (int r = 0; r < nr; ++r) {
+            RingDesc &d = rings[r];
+            d.N = (int)npr[r];
+            d.start = start[r];
+            d.phi0 = phi0[r];
+            if (is_pow2(d.N) && d.N <= 8 * kFftPiece) {
+                d.mode = kDirect;
+                d.P = d.N;
+                d.Q = std::max(1, d.N / kFftPiece);
+                d.bh_off = 0;
             } else {
-                d.bh_off = it->second;
+                d.mode = kBluestein;
+                d.P = (int)next_pow2(2LL * d.N - 1);
+                d.Q = std::max(1, d.P / kFftPiece);
+                if (d.Q > 8) return fail(JHTB_ERR_UNSUPPORTED, "ring length too large (nside > 4096)");
+                auto it = bh_offset.find(d.N);
+                if (it == bh_offset.end()) {
+                    bh_offset[d.N] = bh_len;
+                    blens.push_back(d.N);
+                    boffs.push_back(bh_len);
+                    d.bh_off = bh_len;
+                    bh_len += d.P;
+                } else {
+                    d.bh_off = it->second;
+                }
             }
         }
-    }
-    if ((rc = upload(&p->d_rings, rings, bytes))) return rc;
+        if ((rc = upload(&p->d_rings, rings, bytes))) return rc;
 
-    std::vector<double2> tw(kTwLen);
-    for (int k = 0; k < kTwLen; ++k) {
-        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)kTwLen;
-        tw[k] = make_double2((double)cosl(a), (double)sinl(a));
-    }
-    if ((rc = upload(&p->d_tw, tw, bytes))) return rc;
+        std::vector<double2> tw(kTwLen);
+        for (int k = 0; k < kTwLen; ++k) {
+            long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)kTwLen;
+            tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+        }
+        if ((rc = upload(&p->d_tw, tw, bytes))) return rc;
 
-    p->bh_len = bh_len;
-    JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_bh, sizeof(double2) * std::max(bh_len, 1LL)));
-    bytes += sizeof(double2) * std::max(bh_len, 1LL);
+        p->bh_len = bh_len;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_bh, sizeof(double2) * std::max(bh_len, 1LL)));
+        bytes += sizeof(double2) * std::max(bh_len, 1LL);
+    }
 
     // ---- workspace --------------------------------------------------------------------------
     const size_t f_per_map = sizeof(double2) * (size_t)p->ncomp * nr * M;
@@ -541,6 +543,88 @@ int jhtb_plan_create(int nside, int lmax, int spin, int precision, int max_batch
     return JHTB_OK;
 }
 
+int jhtb_plan_create_rings(int nrings, int lmax, int spin, int precision, int max_batch,
+                           const jhtb_host_tables *tables, jhtb_plan **out) {
+    if (!out) return fail(JHTB_ERR_INVALID, "jhtb_plan_create_rings: out is NULL");
+    *out = nullptr;
+    if (spin != 0 && spin != 2)
+        return fail(JHTB_ERR_UNSUPPORTED, "spin=" + std::to_string(spin) + " unsupported (only 0 and 2)");
+    if (nrings < 1 || nrings > 65535 || nrings % 2 == 0)
+        return fail(JHTB_ERR_INVALID, "nrings must be odd and in [1, 65535], got " + std::to_string(nrings));
+    if (lmax < 0 || lmax > 16383) return fail(JHTB_ERR_INVALID, "lmax must be in [0, 16383]");
+    if (precision == JHTB_PREC_FP32)
+        return fail(JHTB_ERR_UNSUPPORTED, "FP32 contraction is not available in this build");
+    if (precision != JHTB_PREC_FP64 && precision != JHTB_PREC_BF16X3)
+        return fail(JHTB_ERR_INVALID, "unknown precision " + std::to_string(precision));
+    if (max_batch < 1) return fail(JHTB_ERR_INVALID, "max_batch must be >= 1");
+    if (!tables || !tables->x)
+        return fail(JHTB_ERR_INVALID, "jhtb_plan_create_rings: tables->x (the northern rings' cos theta) is required");
+    const int T = (nrings + 1) / 2;
+    for (int t = 0; t < T; ++t) {
+        const double x = tables->x[t];
+        if (!(x >= 0.0 && x <= 1.0) || (t > 0 && x > tables->x[t - 1]))
+            return fail(JHTB_ERR_INVALID, "jhtb_plan_create_rings: x must be non-increasing in [0, 1]");
+    }
+    Plan *p = new (std::nothrow) Plan();
+    if (!p) return fail(JHTB_ERR_NOMEM, "host allocation failed");
+    p->rings_only = true;
+    p->nside = 0;
+    p->lmax = lmax;
+    p->spin = spin;
+    p->precision = precision;
+    p->max_batch = max_batch;
+    p->T = T;
+    p->nrings = nrings;
+    p->M = lmax + 1;
+    p->K = (long long)(lmax + 1) * (lmax + 2) / 2;
+    p->npix = 0;
+    p->ncomp = spin ? 2 : 1;
+    p->npairs = lmax / 2 + 1;
+    int rc = build_plan(p, tables);
+    if (rc) {
+        free_plan(p);
+        return rc;
+    }
+    *out = reinterpret_cast<jhtb_plan *>(p);
+    return JHTB_OK;
+}
+
+int jhtb_legendre_synthesis(jhtb_plan *plan, const void *alm, void *rings, int batch, void *stream) {
+    if (!plan || !alm || !rings) return fail(JHTB_ERR_INVALID, "jhtb_legendre_synthesis: NULL argument");
+    if (batch < 0) return fail(JHTB_ERR_INVALID, "jhtb_legendre_synthesis: negative batch");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    cudaStream_t s = (cudaStream_t)stream;
+    const double2 *a = (const double2 *)alm;
+    double2 *F = (double2 *)rings;
+    const size_t f_map = (size_t)p.ncomp * p.nrings * p.M;
+    for (int b0 = 0; b0 < batch; b0 += p.chunk) {
+        const int nb = std::min(p.chunk, batch - b0);
+        StageTimer t(p, s, kStageLegSynth);
+        const int rc = p.precision == JHTB_PREC_BF16X3
+                           ? launch_tc_synth(p, a + (size_t)b0 * p.ncomp * p.K, F + (size_t)b0 * f_map, nb, s)
+                           : launch_legendre_synth(p, a + (size_t)b0 * p.ncomp * p.K, F + (size_t)b0 * f_map, nb, s);
+        if (rc) return rc;
+    }
+    return JHTB_OK;
+}
+
+int jhtb_legendre_adjoint(jhtb_plan *plan, const void *rings, void *alm, int batch, void *stream) {
+    if (!plan || !alm || !rings) return fail(JHTB_ERR_INVALID, "jhtb_legendre_adjoint: NULL argument");
+    if (batch < 0) return fail(JHTB_ERR_INVALID, "jhtb_legendre_adjoint: negative batch");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    cudaStream_t s = (cudaStream_t)stream;
+    const double2 *F = (const double2 *)rings;
+    double2 *a = (double2 *)alm;
+    const size_t f_map = (size_t)p.ncomp * p.nrings * p.M;
+    for (int b0 = 0; b0 < batch; b0 += p.chunk) {
+        const int nb = std::min(p.chunk, batch - b0);
+        StageTimer t(p, s, kStageLegAdj);
+        const int rc = launch_legendre_adjoint(p, F + (size_t)b0 * f_map, a + (size_t)b0 * p.ncomp * p.K, nb, s);
+        if (rc) return rc;
+    }
+    return JHTB_OK;
+}
+
 int jhtb_plan_destroy(jhtb_plan *plan) {
     free_plan(reinterpret_cast<Plan *>(plan));
     return JHTB_OK;
@@ -556,6 +640,8 @@ int jhtb_synthesis(jhtb_plan *plan, const void *alm, void *maps, int batch, void
     if (!plan || !alm || !maps) return fail(JHTB_ERR_INVALID, "jhtb_synthesis: NULL argument");
     if (batch < 0) return fail(JHTB_ERR_INVALID, "jhtb_synthesis: negative batch");
     Plan &p = *reinterpret_cast<Plan *>(plan);
+    if (p.rings_only)
+        return fail(JHTB_ERR_INVALID, "jhtb_synthesis: a ring-set plan has no pixel grid (use the jhtb_legendre_* calls)");
     cudaStream_t s = (cudaStream_t)stream;
     const double2 *a = (const double2 *)alm;
     double *m = (double *)maps;
@@ -581,6 +667,8 @@ int jhtb_adjoint_synthesis(jhtb_plan *plan, const void *maps, void *alm, int bat
     if (!plan || !alm || !maps) return fail(JHTB_ERR_INVALID, "jhtb_adjoint_synthesis: NULL argument");
     if (batch < 0) return fail(JHTB_ERR_INVALID, "jhtb_adjoint_synthesis: negative batch");
     Plan &p = *reinterpret_cast<Plan *>(plan);
+    if (p.rings_only)
+        return fail(JHTB_ERR_INVALID, "jhtb_adjoint_synthesis: a ring-set plan has no pixel grid (use the jhtb_legendre_* calls)");
     cudaStream_t s = (cudaStream_t)stream;
     const double *m = (const double *)maps;
     double2 *a = (double2 *)alm;
@@ -613,6 +701,7 @@ int jhtb_plan_status(jhtb_plan *plan, int *device_error) {
 int jhtb_plan_ring_costs(const jhtb_plan *plan, int granule, int64_t *cost, int ncost) {
     if (!plan || !cost) return fail(JHTB_ERR_INVALID, "jhtb_plan_ring_costs: NULL argument");
     const Plan &p = *reinterpret_cast<const Plan *>(plan);
+    if (p.rings_only) return fail(JHTB_ERR_INVALID, "jhtb_plan_ring_costs: HEALPix plans only");
     if (granule <= 0 || granule % kRingGranule)
         return fail(JHTB_ERR_INVALID, "jhtb_plan_ring_costs: granule must be a positive multiple of " +
                                           std::to_string(kRingGranule));
@@ -631,6 +720,7 @@ int jhtb_plan_ring_costs(const jhtb_plan *plan, int granule, int64_t *cost, int 
 int jhtb_plan_set_ring_range(jhtb_plan *plan, int t0, int t1) {
     if (!plan) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_ring_range: NULL plan");
     Plan &p = *reinterpret_cast<Plan *>(plan);
+    if (p.rings_only) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_ring_range: HEALPix plans only");
     if (t0 < 0 || t1 > p.T || t0 >= t1 || t0 % kRingGranule || (t1 % kRingGranule && t1 != p.T))
         return fail(JHTB_ERR_INVALID, "jhtb_plan_set_ring_range: need 0 <= t0 < t1 <= 2 nside = " +
                                           std::to_string(p.T) + " with t0 and t1 (unless 2 nside) multiples of " +

@@ -341,7 +341,7 @@ __device__ __forceinline__ void df_add(float &hi, float &lo, float s) {
 template <int SPIN>
 __device__ __forceinline__ void tc_store_F(const TcParams &p, double2 *__restrict__ F_all, int b, int H, int t, int m,
                                            int lmin, const double (&v)[4]) {
-    const size_t rs = (size_t)(4 * p.nside - 2 - t);
+    const size_t rs = (size_t)(p.nrings - 1 - t);
     if (SPIN) {
         const double ssign = ((m + lmin) & 1) ? -1.0 : 1.0;
         double2 *Fp = F_all + (size_t)b * 2 * p.nrings * p.M;

@@ -102,6 +102,7 @@ int jhtb_weighted_residual(const jhtb_plan *plan, const double *maps, const doub
     if (!plan || !maps || !out) return fail(JHTB_ERR_INVALID, "jhtb_weighted_residual: NULL argument");
     if (batch < 0) return fail(JHTB_ERR_INVALID, "jhtb_weighted_residual: negative batch");
     const Plan &p = *reinterpret_cast<const Plan *>(plan);
+    if (p.rings_only) return fail(JHTB_ERR_INVALID, "jhtb_weighted_residual: HEALPix plans only");
     const long long total = (long long)batch * p.ncomp * p.npix;
     if (total == 0) return JHTB_OK;
     weighted_residual_kernel<<<grid_for(total), kVecThreads, 0, (cudaStream_t)stream>>>(maps, synth, ring_w, out,

@@ -172,6 +172,7 @@ def install() -> None:
         "maximum", "minimum", "square", "dot", "vdot", "einsum", "isfinite", "sin", "cos",
     ):
         setattr(jnp, name, getattr(np, name))
+    jnp.iscomplexobj = np.iscomplexobj
     jnp.asarray = lambda a, dtype=None: np.asarray(a, dtype=dtype)
     jnp.array = lambda a, dtype=None: np.array(a, dtype=dtype)
     jnp.zeros = _zeros
@@ -207,8 +208,8 @@ def install() -> None:
 def import_reference(src_dir: str) -> types.ModuleType:
     """Import the reference ``jht`` package from ``src_dir`` without running its ``__init__``.
 
-    The package ``__init__`` pulls in the off-grid NUFFT modules, which are not
-    needed here; the on-grid submodules are imported on demand.
+    The package ``__init__`` would pull in every module at once; the submodules
+    are imported explicitly instead (the off-grid pair ``_nufft`` / ``offgrid`` too).
     """
     import importlib
 
@@ -216,6 +217,7 @@ def import_reference(src_dir: str) -> types.ModuleType:
     pkg = types.ModuleType("jht")
     pkg.__path__ = [f"{src_dir}/jht"]
     sys.modules["jht"] = pkg
-    for sub in ("healpix", "_recursion", "_azimuth", "_analysis", "weights", "masked", "_reference"):
+    for sub in ("healpix", "_recursion", "_azimuth", "_analysis", "weights", "masked", "_reference", "_nufft",
+                "offgrid"):
         setattr(pkg, sub, importlib.import_module(f"jht.{sub}"))
     return pkg

@@ -192,6 +192,50 @@ def main(ref_root: str) -> None:
     np.savez_compressed(HERE / "jht_golden.npz", **out)
     print(f"wrote {len(out)} arrays to {HERE / 'jht_golden.npz'}")
 
+    off = offgrid_fixtures(jht)
+    np.savez_compressed(HERE / "jht_golden_offgrid.npz", **off)
+    print(f"wrote {len(off)} arrays to {HERE / 'jht_golden_offgrid.npz'}")
+
+
+def offgrid_fixtures(jht) -> dict[str, np.ndarray]:
+    """jht's own off-grid ``synthesis_general`` / ``adjoint_synthesis_general`` (offgrid.py)
+    and its NUFFT plan tables (_nufft.py) on seeded inputs."""
+    og, nu = jht.offgrid, jht._nufft
+    out: dict[str, np.ndarray] = {}
+    cases = [
+        # (tag, lmax, spin, npts, epsilon)
+        ("og_s0_l16", 16, 0, 40, 1e-10),
+        ("og_s0_l40", 40, 0, 60, 1e-10),
+        ("og_s2_l16", 16, 2, 40, 1e-10),
+        ("og_s2_l40", 40, 2, 60, 1e-10),
+        ("og_s0_l24_e6", 24, 0, 30, 1e-6),
+        ("og_s2_l24_e12", 24, 2, 30, 1e-12),
+    ]
+    for k, (tag, lmax, spin, npts, eps) in enumerate(cases):
+        rng = np.random.default_rng(6000 + k)
+        loc = np.stack([rng.uniform(0.02, np.pi - 0.02, npts), rng.uniform(0.0, 2.0 * np.pi, npts)], axis=1)
+        # points on the grid's special lines: both poles, phi = 0, the equator
+        loc[:4] = [[0.0, 0.3], [np.pi, 1.1], [0.7, 0.0], [np.pi / 2, 2.0 * np.pi - 1e-9]]
+        if spin == 0:
+            alm = spectrum_alm(rng, lmax)
+            v = rng.standard_normal(npts)
+        else:
+            alm = np.stack([spectrum_alm(rng, lmax, 1.0, 2), spectrum_alm(rng, lmax, 0.1, 2)])
+            v = rng.standard_normal((2, npts))
+        out[f"{tag}/loc"] = loc
+        out[f"{tag}/alm"] = alm
+        out[f"{tag}/field"] = np.asarray(og.synthesis_general(alm, loc, spin=spin, lmax=lmax, epsilon=eps))
+        out[f"{tag}/v"] = v
+        out[f"{tag}/adj"] = np.asarray(og.adjoint_synthesis_general(v, loc, spin=spin, lmax=lmax, epsilon=eps))
+    # NUFFT plan tables: oversampled sizes, kernel width and the deconvolution factors
+    for tag, (Nk, Nm, eps) in {"nu_a": (36, 33, 1e-10), "nu_b": (64, 49, 1e-6)}.items():
+        pl = nu.nufft_plan(Nk, Nm, eps)
+        out[f"{tag}/sizes"] = np.array([pl.nk, pl.nm, pl.W], dtype=np.int64)
+        out[f"{tag}/beta"] = np.array([pl.beta_k, pl.beta_m])
+        out[f"{tag}/corr_k"] = np.asarray(pl.corr_k)
+        out[f"{tag}/corr_m"] = np.asarray(pl.corr_m)
+    return out
+
 
 if __name__ == "__main__":
     main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
