@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mixed-batch", type=int, default=16, help="maps per step of the mixed-precision form (0: skip)")
     ap.add_argument("--mixed-steps", type=int, default=3)
+    ap.add_argument("--offgrid-points", type=int, default=10_000_000,
+                    help="points of the secondary off-grid measurement (0: skip)")
     return ap.parse_args()
 
 
@@ -264,6 +266,39 @@ def run_mixed(args, jhtb, _lib, torch, dev, pg, nside, lmax, spin, rank, world, 
     }
 
 
+def run_offgrid(jhtb, torch, dev, npts: int, lmax: int = 2048, spin: int = 2, reps: int = 3) -> dict:
+    """Secondary line: off-grid synthesis_general and its adjoint (spin 2, lmax 2048) at
+    seeded uniform points, device-resident, CUDA-event timed."""
+    rng = np.random.default_rng(2024)
+    K = jhtb.alm_size(lmax)
+    ell = np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
+    a = (rng.standard_normal((2, K)) + 1j * rng.standard_normal((2, K))) / (ell + 10.0)
+    a[:, : lmax + 1] = a[:, : lmax + 1].real
+    a[:, ell < 2] = 0
+    a = torch.as_tensor(a, device=dev)
+    loc = torch.as_tensor(np.stack([np.arccos(rng.uniform(-1, 1, npts)), rng.uniform(0, 2 * np.pi, npts)], 1),
+                          device=dev)
+    v = torch.as_tensor(rng.standard_normal((2, npts)), device=dev)
+    for _ in range(2):
+        jhtb.synthesis_general(a, loc, spin=spin, lmax=lmax)
+        jhtb.adjoint_synthesis_general(v, loc, spin=spin, lmax=lmax)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    for _ in range(reps):
+        jhtb.synthesis_general(a, loc, spin=spin, lmax=lmax)
+    ev[1].record()
+    for _ in range(reps):
+        jhtb.adjoint_synthesis_general(v, loc, spin=spin, lmax=lmax)
+    ev[2].record()
+    torch.cuda.synchronize()
+    ts, ta = ev[0].elapsed_time(ev[1]) / reps, ev[1].elapsed_time(ev[2]) / reps
+    return {"workload": f"spin-2 synthesis_general / adjoint_synthesis_general, lmax {lmax}, {npts} points "
+                        "uniform on the sphere, epsilon 1e-10 (W = 14)",
+            "synthesis_ms": ts, "adjoint_ms": ta, "synthesis_mpts_per_s": npts / ts / 1e3,
+            "adjoint_mpts_per_s": npts / ta / 1e3}
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
@@ -465,6 +500,8 @@ def main():
             pg.destroy_process_group()
         return
 
+    offgrid = run_offgrid(jhtb, torch, dev, args.offgrid_points) if args.offgrid_points > 0 else None
+
     cpu = None
     if not args.no_cpu_baseline:
         cpu = cpu_baseline(nside, lmax, args.cpu_sample_m)
@@ -506,6 +543,7 @@ def main():
             "synthesis_frac": flops_per_launch / (avg_s * 1e-3) / 1e12 / fp64_peak,
         },
         "mixed": mixed,
+        "offgrid": offgrid,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": sum(n for _, n in stage.values()),
         "clocks": clocks,

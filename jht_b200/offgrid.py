@@ -109,6 +109,22 @@ def _stream():
     return _lib.stream_ptr()
 
 
+_SORT_MIN_POINTS = 1 << 16  # below this the window reads of unsorted points stay in cache
+
+
+def _point_order(g: "_Geometry", theta: torch.Tensor, phi: torch.Tensor):
+    """Permutation that groups the points by 32 x 32-cell tiles of the torus grid, so the
+    windows of neighbouring threads overlap in L1 / L2 (the grid of a large lmax is GBs);
+    None for small point sets."""
+    if theta.numel() < _SORT_MIN_POINTS:
+        return None
+    two_pi = 2.0 * math.pi
+    kb = torch.floor(torch.remainder(torch.nan_to_num(theta), two_pi) * (g.nk / (32.0 * two_pi)))
+    mb = torch.floor(torch.remainder(torch.nan_to_num(phi), two_pi) * (g.nm / (32.0 * two_pi)))
+    key = kb.to(torch.int64) * (g.nm // 32 + 2) + mb.to(torch.int64)
+    return torch.argsort(key)
+
+
 # ---------------------------------------------------------------------------------------
 # forward: alm -> oversampled grid -> points
 # ---------------------------------------------------------------------------------------
@@ -136,6 +152,22 @@ def _torus_grid(g: _Geometry, F: torch.Tensor) -> torch.Tensor:
 
 
 def _interp(g: _Geometry, grid: torch.Tensor, theta: torch.Tensor, phi: torch.Tensor, deriv: bool):
+    order = _point_order(g, theta, phi)
+    if order is not None:
+        out = _interp_raw(g, grid, theta[order], phi[order], deriv)
+        res = []
+        for t in out:
+            if t is None:
+                res.append(None)
+                continue
+            r = torch.empty_like(t)
+            r[order] = t
+            res.append(r)
+        return tuple(res)
+    return _interp_raw(g, grid, theta, phi, deriv)
+
+
+def _interp_raw(g: _Geometry, grid: torch.Tensor, theta: torch.Tensor, phi: torch.Tensor, deriv: bool):
     n = theta.numel()
     out = torch.empty(n, dtype=torch.complex128, device=theta.device)
     dth = torch.empty_like(out) if deriv else None
@@ -164,6 +196,9 @@ def _adjoint(g: _Geometry, fc: torch.Tensor, theta: torch.Tensor, phi: torch.Ten
     divided by the metric (offgrid.py:223-243)."""
     L, ns, nd = g.lmax, g.ns, g.nd
     grid = torch.zeros((g.nk, g.nm), dtype=torch.complex128, device=fc.device)
+    order = _point_order(g, theta, phi)
+    if order is not None:
+        fc, theta, phi = fc[order], theta[order], phi[order]
     st = g.plan.lib.jhtb_nufft_spread(fc.contiguous().data_ptr(), theta.data_ptr(), phi.data_ptr(), theta.numel(),
                                       g.nk, g.nm, g.W, ctypes.c_double(g.beta), grid.data_ptr(), _stream())
     _lib.check(st, "jhtb_nufft_spread")

@@ -80,7 +80,7 @@ def test_offgrid_matches_oracle_and_direct_sum(spin, lmax, npts):
 
 @pytest.mark.parametrize("spin", [0, 2])
 def test_offgrid_adjoint_identity(spin):
-    lmax, npts = 300, 5000
+    lmax, npts = 300, 200_000  # enough points for the tile-sorted path
     rng = np.random.default_rng(31 + spin)
     alm, loc = _alm(rng, lmax, spin), _loc(rng, npts)
     v = rng.standard_normal(npts) if spin == 0 else rng.standard_normal((2, npts))
