@@ -16,7 +16,7 @@ from __future__ import annotations
 from ._analysis import analysis, bare_analysis, map2alm
 from ._azimuth import enable_looped_fft, get_azimuth_fft_mode, set_azimuth_fft_mode
 from ._cache import enable_compilation_cache
-from .diff import analysis_real, bandpower, synthesis_real
+from .diff import adjoint_synthesis_general_real, analysis_real, bandpower, synthesis_general_real, synthesis_real
 from .healpix import (
     adjoint_synthesis,
     adjoint_synthesis_batch,
@@ -58,6 +58,8 @@ __all__ = [
     "adjoint_synthesis_general",
     "synthesis_real",
     "analysis_real",
+    "synthesis_general_real",
+    "adjoint_synthesis_general_real",
     "bandpower",
     "alm_to_real",
     "real_to_alm",

@@ -15,8 +15,10 @@ import torch
 from ._analysis import analysis
 from .healpix import alm_metric_weight, synthesis
 from .masked import alm_to_real, n_dof, real_to_alm
+from .offgrid import adjoint_synthesis_general, synthesis_general
 
-__all__ = ["synthesis_real", "analysis_real", "bandpower", "alm_to_real", "real_to_alm", "n_dof"]
+__all__ = ["synthesis_real", "analysis_real", "synthesis_general_real", "adjoint_synthesis_general_real", "bandpower",
+           "alm_to_real", "real_to_alm", "n_dof"]
 
 
 def synthesis_real(x, nside: int, lmax: int, spin: int = 0, *, precision: str = "fp64") -> torch.Tensor:
@@ -32,6 +34,18 @@ def analysis_real(maps, nside: int, lmax: int, spin: int = 0, niter: int = 3, us
 
 
 @lru_cache(maxsize=None)
+def synthesis_general_real(x, loc, *, spin: int = 0, lmax: int, epsilon: float = 1e-10) -> torch.Tensor:
+    """``S_g o T^-1``: real DOF vector -> field at the points ``loc`` (diff.py:79-92); a plain
+    real-linear map, differentiable in ``x`` and ``loc``."""
+    return synthesis_general(real_to_alm(x, lmax, spin), loc, spin=spin, lmax=lmax, epsilon=epsilon)
+
+
+def adjoint_synthesis_general_real(field, loc, *, spin: int = 0, lmax: int, epsilon: float = 1e-10) -> torch.Tensor:
+    """``T o S_g^T``: field at ``loc`` -> real DOF vector, the Euclidean transpose of
+    :func:`synthesis_general_real` (diff.py:95-107)."""
+    return alm_to_real(adjoint_synthesis_general(field, loc, spin=spin, lmax=lmax, epsilon=epsilon), lmax, spin)
+
+
 def _ell_of_idx(lmax: int) -> np.ndarray:
     return np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
 
