@@ -34,7 +34,7 @@ __all__ = ["bare_analysis", "analysis", "map2alm"]
 
 @lru_cache(maxsize=None)
 def _ring_w_device(nside: int, device_index: int) -> torch.Tensor:
-    return torch.as_tensor(np.asarray(ring_weights(nside)), device=torch.device("cuda", device_index))
+    return torch.as_tensor(np.array(ring_weights(nside)), device=torch.device("cuda", device_index))
 
 
 @lru_cache(maxsize=None)

@@ -33,7 +33,6 @@ def analysis_real(maps, nside: int, lmax: int, spin: int = 0, niter: int = 3, us
     return alm_to_real(a, lmax, spin)
 
 
-@lru_cache(maxsize=None)
 def synthesis_general_real(x, loc, *, spin: int = 0, lmax: int, epsilon: float = 1e-10) -> torch.Tensor:
     """``S_g o T^-1``: real DOF vector -> field at the points ``loc`` (diff.py:79-92); a plain
     real-linear map, differentiable in ``x`` and ``loc``."""
@@ -46,6 +45,7 @@ def adjoint_synthesis_general_real(field, loc, *, spin: int = 0, lmax: int, epsi
     return alm_to_real(adjoint_synthesis_general(field, loc, spin=spin, lmax=lmax, epsilon=epsilon), lmax, spin)
 
 
+@lru_cache(maxsize=None)
 def _ell_of_idx(lmax: int) -> np.ndarray:
     return np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
 
