@@ -176,6 +176,17 @@ int jhtb_nufft_interp(const void *grid, int nk, int nm, int W, double beta, cons
 int jhtb_nufft_spread(const void *vals, const double *theta, const double *phi, int64_t npts, int nk,
                       int nm, int W, double beta, void *grid, void *stream);
 
+/* jhtb_nufft_spread for points grouped by 32 x 32-cell tiles of the grid: segment i covers
+ * points [seg_start[i], seg_start[i] + seg_count[i]) (inside [0, npts)), all keyed to tile
+ * seg_tile[i] = kb * tiles_m + mb (rows kb = floor(theta nk / (64 pi)), columns
+ * mb = floor(phi nm / (64 pi))).  Each segment's windows are summed in on-chip memory and
+ * added to the grid once per cell; a point outside its segment's tile is added directly.
+ * Same result as jhtb_nufft_spread up to the order of the sums. */
+int jhtb_nufft_spread_tiles(const void *vals, const double *theta, const double *phi, int64_t npts,
+                            int64_t nseg, const int64_t *seg_start, const int *seg_count,
+                            const int64_t *seg_tile, int tiles_m, int nk, int nm, int W, double beta,
+                            void *grid, void *stream);
+
 /* ---- sharding over devices (no counterpart in jht, which runs on one device) ----
  * A plan can be restricted to the ring pairs of half-grid rings [t0, t1) (the
  * northern rings t0..t1-1, the equator included when t1 = 2 nside, and their

@@ -50,6 +50,7 @@ EXPORTS = (
     "jhtb_legendre_adjoint",
     "jhtb_nufft_interp",
     "jhtb_nufft_spread",
+    "jhtb_nufft_spread_tiles",
 )
 
 
@@ -111,6 +112,8 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_legendre_adjoint": (i32, [vp, vp, vp, i32, vp]),
             "jhtb_nufft_interp": (i32, [vp, i32, i32, i32, ctypes.c_double, dp, dp, i64, vp, vp, vp, vp]),
             "jhtb_nufft_spread": (i32, [vp, dp, dp, i64, i32, i32, i32, ctypes.c_double, vp, vp]),
+            "jhtb_nufft_spread_tiles": (i32, [vp, dp, dp, i64, i64, vp, vp, vp, i32, i32, i32, i32, ctypes.c_double,
+                                              vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)

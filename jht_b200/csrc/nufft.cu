@@ -134,6 +134,76 @@ __global__ void __launch_bounds__(kNuThreads) spread_kernel(const double2 *__res
     }
 }
 
+// Tiled spread: the points arrive grouped by kTile x kTile-cell tiles of the grid (segments
+// of one tile, at most kSegPoints points each).  A CTA adds its segment's windows into a
+// shared-memory copy of the tile plus its W-cell halo, then adds that block to the grid once
+// per cell, so the global atomics fall from 2 W^2 per point to 2 (kTile + W)^2 per segment.
+// A point whose window leaves the block (a coordinate outside the tile its key named) is
+// added straight to the grid.
+constexpr int kTile = 32;
+constexpr int kSpreadThreads = 128;
+
+template <int W>
+__global__ void __launch_bounds__(kSpreadThreads) spread_tiles_kernel(
+    const double2 *__restrict__ vals, const double *__restrict__ theta, const double *__restrict__ phi,
+    long long npts, const long long *__restrict__ seg_start, const int *__restrict__ seg_count,
+    const long long *__restrict__ seg_tile, int tiles_m, int nk, int nm, double beta, double2 *__restrict__ grid) {
+    constexpr int B = kTile + W;  // block edge: the tile and its halo
+    __shared__ double acc[B * B * 2];
+    for (int i = threadIdx.x; i < B * B * 2; i += blockDim.x) acc[i] = 0.0;
+    __syncthreads();
+    const long long seg = blockIdx.x;
+    const long long tile = seg_tile[seg];
+    const long long k_org = (tile / tiles_m) * kTile - W / 2, m_org = (tile % tiles_m) * kTile - W / 2;
+    const long long p0 = seg_start[seg];
+    const int cnt = seg_count[seg];
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+        const long long j = p0 + q;
+        if (j < 0 || j >= npts) continue;
+        long long k0, m0;
+        double wk[W], wm[W], unused[W];
+        window<W, false>(theta[j], nk, beta, k0, wk, unused);
+        window<W, false>(phi[j], nm, beta, m0, wm, unused);
+        const double2 v = vals[j];
+        const long long lk = k0 - k_org, lm = m0 - m_org;
+        if (lk >= 0 && lk + W <= B && lm >= 0 && lm + W <= B) {
+#pragma unroll 1
+            for (int a = 0; a < W; ++a) {
+                double *row = acc + 2 * ((lk + a) * B + lm);
+                const double vx = wk[a] * v.x, vy = wk[a] * v.y;
+#pragma unroll
+                for (int b = 0; b < W; ++b) {
+                    atomicAdd(row + 2 * b, wm[b] * vx);
+                    atomicAdd(row + 2 * b + 1, wm[b] * vy);
+                }
+            }
+        } else {
+            int mi[W];
+#pragma unroll
+            for (int b = 0; b < W; ++b) mi[b] = wrap(m0 + b, nm);
+#pragma unroll 1
+            for (int a = 0; a < W; ++a) {
+                double *row = reinterpret_cast<double *>(grid + (size_t)wrap(k0 + a, nk) * nm);
+                const double vx = wk[a] * v.x, vy = wk[a] * v.y;
+#pragma unroll
+                for (int b = 0; b < W; ++b) {
+                    atomicAdd(row + 2 * mi[b], wm[b] * vx);
+                    atomicAdd(row + 2 * mi[b] + 1, wm[b] * vy);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < B * B; c += blockDim.x) {
+        const double x = acc[2 * c], y = acc[2 * c + 1];
+        if (x == 0.0 && y == 0.0) continue;
+        const int a = c / B, b = c - a * B;
+        double *cell = reinterpret_cast<double *>(grid + (size_t)wrap(k_org + a, nk) * nm + wrap(m_org + b, nm));
+        atomicAdd(cell, x);
+        atomicAdd(cell + 1, y);
+    }
+}
+
 int grid_blocks(long long npts) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -163,6 +233,14 @@ template <int W>
 void launch_spread(const double2 *v, const double *th, const double *ph, long long n, int nk, int nm, double beta,
                    double2 *g, cudaStream_t s) {
     spread_kernel<W><<<grid_blocks(n), kNuThreads, 0, s>>>(v, th, ph, n, nk, nm, beta, g);
+}
+
+template <int W>
+void launch_spread_tiles(const double2 *v, const double *th, const double *ph, long long npts, long long nseg,
+                         const long long *start, const int *count, const long long *tile, int tiles_m, int nk, int nm,
+                         double beta, double2 *g, cudaStream_t s) {
+    spread_tiles_kernel<W><<<(unsigned)nseg, kSpreadThreads, 0, s>>>(v, th, ph, npts, start, count, tile, tiles_m, nk,
+                                                                    nm, beta, g);
 }
 
 }  // namespace
@@ -209,6 +287,33 @@ int jhtb_nufft_spread(const void *vals, const double *theta, const double *phi, 
         case 10: launch_spread<10>(v, theta, phi, npts, nk, nm, beta, g, s); break;
         case 14: launch_spread<14>(v, theta, phi, npts, nk, nm, beta, g, s); break;
         default: launch_spread<16>(v, theta, phi, npts, nk, nm, beta, g, s); break;
+    }
+    JHTB_CUDA_TRY(cudaGetLastError());
+    return JHTB_OK;
+}
+
+int jhtb_nufft_spread_tiles(const void *vals, const double *theta, const double *phi, int64_t npts, int64_t nseg,
+                            const int64_t *seg_start, const int *seg_count, const int64_t *seg_tile, int tiles_m,
+                            int nk, int nm, int W, double beta, void *grid, void *stream) {
+    if (!vals || !theta || !phi || !grid || (nseg > 0 && (!seg_start || !seg_count || !seg_tile)))
+        return fail(JHTB_ERR_INVALID, "jhtb_nufft_spread_tiles: NULL argument");
+    int rc = check_args(nk, nm, W, npts, "jhtb_nufft_spread_tiles");
+    if (rc) return rc;
+    rc = nseg < 0 ? fail(JHTB_ERR_INVALID, "jhtb_nufft_spread_tiles: negative segment count") : JHTB_OK;
+    if (rc) return rc;
+    if (tiles_m < 1) return fail(JHTB_ERR_INVALID, "jhtb_nufft_spread_tiles: tiles_m must be >= 1");
+    if (nseg > 0x7fffffffLL) return fail(JHTB_ERR_INVALID, "jhtb_nufft_spread_tiles: too many segments");
+    if (nseg == 0) return JHTB_OK;
+    const double2 *v = (const double2 *)vals;
+    double2 *g = (double2 *)grid;
+    const long long *st = (const long long *)seg_start, *tl = (const long long *)seg_tile;
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (W) {
+        case 6: launch_spread_tiles<6>(v, theta, phi, npts, nseg, st, seg_count, tl, tiles_m, nk, nm, beta, g, s); break;
+        case 8: launch_spread_tiles<8>(v, theta, phi, npts, nseg, st, seg_count, tl, tiles_m, nk, nm, beta, g, s); break;
+        case 10: launch_spread_tiles<10>(v, theta, phi, npts, nseg, st, seg_count, tl, tiles_m, nk, nm, beta, g, s); break;
+        case 14: launch_spread_tiles<14>(v, theta, phi, npts, nseg, st, seg_count, tl, tiles_m, nk, nm, beta, g, s); break;
+        default: launch_spread_tiles<16>(v, theta, phi, npts, nseg, st, seg_count, tl, tiles_m, nk, nm, beta, g, s); break;
     }
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;

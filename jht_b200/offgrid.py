@@ -85,6 +85,7 @@ class _Geometry:
         self.Nm = 2 * lmax + 1
         self.nk, self.nm = _fft_size(sigma * self.nd), _fft_size(sigma * self.Nm)
         self.beta = float(np.pi * self.W * (1.0 - 0.5 / sigma))
+        self.tiles_m = self.nm // _TILE + 2
         dev = torch.device("cuda", device)
         ck = _kernel_ft(self.nd, self.nk, self.W, self.beta)
         cm = _kernel_ft(self.Nm, self.nm, self.W, self.beta)
@@ -112,17 +113,41 @@ def _stream():
 _SORT_MIN_POINTS = 1 << 16  # below this the window reads of unsorted points stay in cache
 
 
+_TILE = 32  # grid cells per tile edge (kTile in nufft.cu)
+_SEG_POINTS = 1024  # points per spread segment
+
+
+def _tile_keys(g: "_Geometry", theta: torch.Tensor, phi: torch.Tensor) -> torch.Tensor:
+    two_pi = 2.0 * math.pi
+    kb = torch.floor(torch.remainder(torch.nan_to_num(theta), two_pi) * (g.nk / (_TILE * two_pi)))
+    mb = torch.floor(torch.remainder(torch.nan_to_num(phi), two_pi) * (g.nm / (_TILE * two_pi)))
+    return kb.to(torch.int64) * g.tiles_m + mb.to(torch.int64)
+
+
 def _point_order(g: "_Geometry", theta: torch.Tensor, phi: torch.Tensor):
-    """Permutation that groups the points by 32 x 32-cell tiles of the torus grid, so the
-    windows of neighbouring threads overlap in L1 / L2 (the grid of a large lmax is GBs);
-    None for small point sets."""
+    """(permutation, sorted tile keys) grouping the points by 32 x 32-cell tiles of the
+    torus grid, so neighbouring threads' windows overlap in L1 / L2 (the grid of a large
+    lmax is GBs); None for small point sets."""
     if theta.numel() < _SORT_MIN_POINTS:
         return None
-    two_pi = 2.0 * math.pi
-    kb = torch.floor(torch.remainder(torch.nan_to_num(theta), two_pi) * (g.nk / (32.0 * two_pi)))
-    mb = torch.floor(torch.remainder(torch.nan_to_num(phi), two_pi) * (g.nm / (32.0 * two_pi)))
-    key = kb.to(torch.int64) * (g.nm // 32 + 2) + mb.to(torch.int64)
-    return torch.argsort(key)
+    key = _tile_keys(g, theta, phi)
+    ks, order = torch.sort(key)
+    return order, ks
+
+
+def _segments(sorted_keys: torch.Tensor):
+    """Segments of at most _SEG_POINTS consecutive sorted points within one tile:
+    (first point, count, tile key)."""
+    tiles, counts = torch.unique_consecutive(sorted_keys, return_counts=True)
+    starts = torch.cumsum(counts, 0) - counts
+    nseg = (counts + _SEG_POINTS - 1) // _SEG_POINTS
+    seg_tile = torch.repeat_interleave(tiles, nseg)
+    first_seg = torch.cumsum(nseg, 0) - nseg
+    within = torch.arange(seg_tile.numel(), device=sorted_keys.device) - torch.repeat_interleave(first_seg, nseg)
+    seg_start = torch.repeat_interleave(starts, nseg) + within * _SEG_POINTS
+    seg_end = torch.repeat_interleave(starts + counts, nseg)
+    seg_count = torch.minimum(seg_end - seg_start, torch.full_like(seg_start, _SEG_POINTS)).to(torch.int32)
+    return seg_start.contiguous(), seg_count.contiguous(), seg_tile.contiguous()
 
 
 # ---------------------------------------------------------------------------------------
@@ -152,8 +177,9 @@ def _torus_grid(g: _Geometry, F: torch.Tensor) -> torch.Tensor:
 
 
 def _interp(g: _Geometry, grid: torch.Tensor, theta: torch.Tensor, phi: torch.Tensor, deriv: bool):
-    order = _point_order(g, theta, phi)
-    if order is not None:
+    po = _point_order(g, theta, phi)
+    if po is not None:
+        order = po[0]
         out = _interp_raw(g, grid, theta[order], phi[order], deriv)
         res = []
         for t in out:
@@ -196,12 +222,20 @@ def _adjoint(g: _Geometry, fc: torch.Tensor, theta: torch.Tensor, phi: torch.Ten
     divided by the metric (offgrid.py:223-243)."""
     L, ns, nd = g.lmax, g.ns, g.nd
     grid = torch.zeros((g.nk, g.nm), dtype=torch.complex128, device=fc.device)
-    order = _point_order(g, theta, phi)
-    if order is not None:
-        fc, theta, phi = fc[order], theta[order], phi[order]
-    st = g.plan.lib.jhtb_nufft_spread(fc.contiguous().data_ptr(), theta.data_ptr(), phi.data_ptr(), theta.numel(),
-                                      g.nk, g.nm, g.W, ctypes.c_double(g.beta), grid.data_ptr(), _stream())
-    _lib.check(st, "jhtb_nufft_spread")
+    po = _point_order(g, theta, phi)
+    if po is not None:
+        order, keys = po
+        fc, theta, phi = fc[order].contiguous(), theta[order].contiguous(), phi[order].contiguous()
+        seg_start, seg_count, seg_tile = _segments(keys)
+        st = g.plan.lib.jhtb_nufft_spread_tiles(
+            fc.data_ptr(), theta.data_ptr(), phi.data_ptr(), theta.numel(), seg_start.numel(), seg_start.data_ptr(),
+            seg_count.data_ptr(), seg_tile.data_ptr(), g.tiles_m, g.nk, g.nm, g.W, ctypes.c_double(g.beta),
+            grid.data_ptr(), _stream())
+        _lib.check(st, "jhtb_nufft_spread_tiles")
+    else:
+        st = g.plan.lib.jhtb_nufft_spread(fc.contiguous().data_ptr(), theta.data_ptr(), phi.data_ptr(), theta.numel(),
+                                          g.nk, g.nm, g.W, ctypes.c_double(g.beta), grid.data_ptr(), _stream())
+        _lib.check(st, "jhtb_nufft_spread")
     G = torch.fft.fft2(grid)[g.kpos[:, None], g.mpos[None, :]] * g.inv_corr
     d = torch.fft.ifft(torch.fft.ifftshift(G, dim=0), dim=0)
     top = d[:ns].clone()

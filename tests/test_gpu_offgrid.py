@@ -167,3 +167,35 @@ def test_offgrid_rejects_bad_inputs():
         jhtb.adjoint_synthesis_general(np.zeros(4, complex), loc, spin=0, lmax=4)
     with pytest.raises(ValueError, match="field shape"):
         jhtb.adjoint_synthesis_general(np.zeros(5), loc, spin=0, lmax=4)
+
+
+def test_tiled_spread_equals_plain_spread():
+    """jhtb_nufft_spread_tiles (per-tile sums in on-chip memory) against jhtb_nufft_spread on
+    the same points, including points whose coordinates lie outside [0, 2 pi) (their tile
+    key names another tile, so they take the direct path)."""
+    import ctypes
+
+    from jht_b200 import _lib, offgrid
+
+    g = offgrid._geometry(64, 0, 1e-10, torch.cuda.current_device())
+    rng = np.random.default_rng(3)
+    n = 100_000
+    th = rng.uniform(0, np.pi, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    th[:50] = rng.uniform(-3.0, -0.1, 50)
+    ph[50:100] = rng.uniform(6.5, 9.0, 50)
+    theta = torch.as_tensor(th, device="cuda")
+    phi = torch.as_tensor(ph, device="cuda")
+    vals = torch.complex(torch.randn(n, dtype=torch.float64, device="cuda"), torch.randn(n, dtype=torch.float64, device="cuda"))
+    ks, order = torch.sort(offgrid._tile_keys(g, theta, phi))
+    theta, phi, vals = theta[order].contiguous(), phi[order].contiguous(), vals[order].contiguous()
+    s0, c0, t0 = offgrid._segments(ks)
+    lib = _lib.load_library()
+    g1 = torch.zeros((g.nk, g.nm), dtype=torch.complex128, device="cuda")
+    g2 = torch.zeros_like(g1)
+    _lib.check(lib.jhtb_nufft_spread(vals.data_ptr(), theta.data_ptr(), phi.data_ptr(), n, g.nk, g.nm, g.W,
+                                     ctypes.c_double(g.beta), g1.data_ptr(), _lib.stream_ptr()), "spread")
+    _lib.check(lib.jhtb_nufft_spread_tiles(vals.data_ptr(), theta.data_ptr(), phi.data_ptr(), n, s0.numel(),
+                                           s0.data_ptr(), c0.data_ptr(), t0.data_ptr(), g.tiles_m, g.nk, g.nm, g.W,
+                                           ctypes.c_double(g.beta), g2.data_ptr(), _lib.stream_ptr()), "spread_tiles")
+    assert float(torch.max(torch.abs(g1 - g2))) <= 1e-12 * float(torch.max(torch.abs(g1)))
