@@ -27,6 +27,7 @@
  *   jhtb_legendre_adjoint   offgrid.py:163-168 (adjoint_contract at those rings)
  *   jhtb_nufft_interp       _nufft.py:164-178 (nufft2d2's window sums)
  *   jhtb_nufft_spread       _nufft.py:181-188 (nufft2d1's scatter-add)
+ *   jhtb_nufft_spread_tiles _nufft.py:181-188 (the same, for points grouped by grid tile)
  */
 #ifndef JHTB_H
 #define JHTB_H
