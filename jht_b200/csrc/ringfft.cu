@@ -22,7 +22,14 @@
 namespace jhtb {
 namespace {
 
-constexpr int kFftThreads = 256;
+#ifndef JHTB_FFT_THREADS
+#define JHTB_FFT_THREADS 256
+#endif
+#ifndef JHTB_FFT_MINB
+#define JHTB_FFT_MINB 2
+#endif
+constexpr int kFftThreads = JHTB_FFT_THREADS;  // threads per ring CTA
+constexpr int kFftMinBlocks = JHTB_FFT_MINB;   // resident ring CTAs per SM (4096-point buffers)
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -142,11 +149,11 @@ __device__ __forceinline__ void reg_fft(double2 (&v)[R], double dir) {
 // radices): every thread loads its R inputs (stride n/R), twiddles them by
 // e^{dir 2 pi i (j mod Ns) r / (Ns R)}, runs an R-point DFT in registers and, after a
 // barrier, stores them at (j / Ns) Ns R + (j mod Ns) + r Ns.  n <= kFftPiece = 4096
-// and 256 threads: each thread holds at most 16 points.
+// and kFftThreads threads: each thread holds at most kFftPiece / kFftThreads points.
 template <int R>
 __device__ __forceinline__ void stockham_pass(double2 *buf, int n, int Ns, double dir,
                                               const double2 *__restrict__ tw) {
-    constexpr int JM = 16 / R;
+    constexpr int JM = kFftPiece / (R * kFftThreads);
     const int nj = n / R;
     double2 v[JM][R];
 #pragma unroll
@@ -235,7 +242,7 @@ __device__ __forceinline__ double2 fold_synth(const double2 *__restrict__ Fp, co
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, 2) ring_synth_kernel(const int *__restrict__ ring_list,
+__global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(const int *__restrict__ ring_list,
                                                                      const RingDesc *__restrict__ rings, int lmax,
                                                                      int M, int nrings, long long npix,
                                                                      const double2 *__restrict__ F_all,
@@ -343,7 +350,7 @@ __device__ __forceinline__ void gather_adjoint(const double2 *W, int N, int lmax
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, 2) ring_adjoint_kernel(const int *__restrict__ ring_list,
+__global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kernel(const int *__restrict__ ring_list,
                                                                        const RingDesc *__restrict__ rings, int lmax,
                                                                        int M, int nrings, long long npix,
                                                                        const double *__restrict__ maps_all,
