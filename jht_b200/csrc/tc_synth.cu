@@ -40,7 +40,13 @@ namespace {
 
 constexpr int kTcRows = 128;     // = MMA M = rings per tile
 constexpr int kTcK = 16;         // l steps per chunk = MMA K (BF16)
-constexpr int kFlush = 16;       // chunks per FP32 accumulation block (256 l)
+#ifndef JHTB_TC_FLUSH
+#define JHTB_TC_FLUSH 16
+#endif
+#ifndef JHTB_TC_NSA
+#define JHTB_TC_NSA 2
+#endif
+constexpr int kFlush = JHTB_TC_FLUSH;  // chunks per FP32 accumulation block (256 l)
 constexpr unsigned kWaitLimit = 1u << 26;
 
 // ---------------------------------------------------------------------------------
@@ -210,7 +216,7 @@ struct TcCfg {
     static constexpr int NBW = kTcK * BM / 32;      // builder warps: one thread per (l, map) of a chunk
     static constexpr int MMA_WARP = NPW + NBW;
     static constexpr int NTHREADS = (NPW + NBW + 1) * 32;
-    static constexpr int NSA = 2;                   // A stages (in tensor memory)
+    static constexpr int NSA = JHTB_TC_NSA;         // A stages (in tensor memory)
     static constexpr int NSB = 4;                   // B stages (with the chunk's coefficients)
     static constexpr int BTILE = N * kTcK * 2;
     static constexpr int ACOLS = kTcK / 2;          // tensor-memory columns of one A row (16 BF16)
