@@ -187,3 +187,35 @@ def test_no_cpu_fallback():
         jhtb.adjoint_synthesis(np.zeros(768), 8, 8, 0)
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         jhtb.analysis(np.zeros(768), 8, 8, 0)
+
+
+def test_ring_set_plan_validates_before_device_work(lib):
+    x = np.array([1.0, 0.7, 0.2, 0.0])
+    ht = _lib.HostTables(x.ctypes.data, None, None, None, None)
+    h = ctypes.c_void_p()
+    # even ring count, bad spin, missing x, increasing x
+    assert lib.jhtb_plan_create_rings(8, 16, 0, 0, 1, ctypes.byref(ht), ctypes.byref(h)) == _lib.JHTB_ERR_INVALID
+    assert "odd" in _lib.last_error()
+    assert lib.jhtb_plan_create_rings(7, 16, 1, 0, 1, ctypes.byref(ht), ctypes.byref(h)) == _lib.JHTB_ERR_UNSUPPORTED
+    assert lib.jhtb_plan_create_rings(7, 16, 0, 0, 1, None, ctypes.byref(h)) == _lib.JHTB_ERR_INVALID
+    bad = np.array([0.2, 0.7, 1.0, 0.0])
+    ht_bad = _lib.HostTables(bad.ctypes.data, None, None, None, None)
+    assert lib.jhtb_plan_create_rings(7, 16, 0, 0, 1, ctypes.byref(ht_bad), ctypes.byref(h)) == _lib.JHTB_ERR_INVALID
+    assert "non-increasing" in _lib.last_error()
+    assert h.value is None
+
+
+def test_nufft_calls_validate_before_device_work(lib):
+    one = ctypes.c_void_p(16)  # never dereferenced: every call below fails its argument checks
+    d = ctypes.c_double(1.0)
+    assert lib.jhtb_nufft_interp(None, 8, 8, 14, d, None, None, 4, None, None, None, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_nufft_interp(one, 8, 8, 7, d, one, one, 4, one, None, None, None) == _lib.JHTB_ERR_UNSUPPORTED
+    assert lib.jhtb_nufft_interp(one, 8, 8, 14, d, one, one, 4, one, one, None, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_nufft_spread(one, one, one, -1, 8, 8, 14, d, one, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_nufft_spread(one, one, one, 4, 0, 8, 14, d, one, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_nufft_spread_tiles(one, one, one, 4, 2, None, None, None, 4, 8, 8, 14, d, one, None) == \
+        _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_nufft_spread_tiles(one, one, one, 4, -1, one, one, one, 4, 8, 8, 14, d, one, None) == \
+        _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_legendre_synthesis(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_legendre_adjoint(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
