@@ -82,3 +82,36 @@ def test_offgrid_validation_errors_without_gpu():
         jhtb.synthesis_general(np.zeros(jhtb.alm_size(4), complex), np.zeros((3, 2)), spin=1, lmax=4)
     with pytest.raises(ValueError, match="loc must have shape"):
         jhtb.synthesis_general(np.zeros(jhtb.alm_size(4), complex), np.zeros((3, 3)), spin=0, lmax=4)
+
+
+def test_tile_segments_cover_every_sorted_point_once():
+    """Host-side grouping of the points for the tiled spread: segments of one tile each,
+    at most _SEG_POINTS long, covering the sorted points exactly once in order."""
+    import types
+
+    import torch
+
+    from jht_b200 import offgrid
+
+    g = types.SimpleNamespace(nk=8640, nm=8640, tiles_m=8640 // 32 + 2)
+    rng = np.random.default_rng(7)
+    n = 50_000
+    th = np.concatenate([rng.uniform(0, np.pi, n - 3000), np.full(3000, 0.5)])  # one crowded tile
+    ph = np.concatenate([rng.uniform(0, 2 * np.pi, n - 3000), np.full(3000, 1.0)])
+    th[:5] = [-0.3, 7.0, np.nan, 0.0, np.pi]
+    keys = offgrid._tile_keys(g, torch.as_tensor(th), torch.as_tensor(ph))
+    assert int(keys.min()) >= 0
+    ks, order = torch.sort(keys)
+    start, count, tile = offgrid._segments(ks)
+    assert int(count.max()) <= offgrid._SEG_POINTS
+    assert int(count.min()) >= 1
+    ends = start + count.to(torch.int64)
+    assert int(start[0]) == 0 and int(ends[-1]) == n
+    assert torch.equal(start[1:], ends[:-1])  # contiguous, in order, no overlap
+    for i in rng.choice(start.numel(), 50, replace=False):
+        seg = ks[int(start[i]) : int(ends[i])]
+        assert bool(torch.all(seg == tile[i]))
+    crowded = int(offgrid._tile_keys(g, torch.tensor([0.5]), torch.tensor([1.0]))[0])
+    n_crowded = int((ks == crowded).sum())
+    assert n_crowded >= 3000
+    assert int((tile == crowded).sum()) == -(-n_crowded // offgrid._SEG_POINTS)
