@@ -516,7 +516,7 @@ int jhtb_plan_create(int nside, int lmax, int spin, int precision, int max_batch
         return fail(JHTB_ERR_INVALID, "nside must be in [1, 4096], got " + std::to_string(nside));
     if (lmax < 0 || lmax > 16383) return fail(JHTB_ERR_INVALID, "lmax must be in [0, 16383]");
     if (precision == JHTB_PREC_FP32)
-        return fail(JHTB_ERR_UNSUPPORTED, "FP32 contraction is not available in this build");
+        return fail(JHTB_ERR_UNSUPPORTED, "FP32 contraction is not implemented (use JHTB_PREC_FP64 or JHTB_PREC_BF16X3)");
     if (precision != JHTB_PREC_FP64 && precision != JHTB_PREC_BF16X3)
         return fail(JHTB_ERR_INVALID, "unknown precision " + std::to_string(precision));
     if (max_batch < 1) return fail(JHTB_ERR_INVALID, "max_batch must be >= 1");
@@ -553,7 +553,7 @@ int jhtb_plan_create_rings(int nrings, int lmax, int spin, int precision, int ma
         return fail(JHTB_ERR_INVALID, "nrings must be odd and in [1, 65535], got " + std::to_string(nrings));
     if (lmax < 0 || lmax > 16383) return fail(JHTB_ERR_INVALID, "lmax must be in [0, 16383]");
     if (precision == JHTB_PREC_FP32)
-        return fail(JHTB_ERR_UNSUPPORTED, "FP32 contraction is not available in this build");
+        return fail(JHTB_ERR_UNSUPPORTED, "FP32 contraction is not implemented (use JHTB_PREC_FP64 or JHTB_PREC_BF16X3)");
     if (precision != JHTB_PREC_FP64 && precision != JHTB_PREC_BF16X3)
         return fail(JHTB_ERR_INVALID, "unknown precision " + std::to_string(precision));
     if (max_batch < 1) return fail(JHTB_ERR_INVALID, "max_batch must be >= 1");

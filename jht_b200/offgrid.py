@@ -323,7 +323,7 @@ def _check_spin(spin: int) -> None:
     if spin not in (0, 1, 2, 3):
         raise NotImplementedError(f"spin={spin} unsupported (0, 1, 2, 3)")
     if spin not in (0, 2):
-        raise NotImplementedError(f"spin={spin}: this build implements the off-grid transforms for spin 0 and 2")
+        raise NotImplementedError(f"spin={spin}: the off-grid transforms are implemented for spin 0 and 2")
 
 
 def synthesis_general(alm, loc, *, spin: int = 0, lmax: int, epsilon: float = 1e-10) -> torch.Tensor:
