@@ -219,3 +219,22 @@ def test_nufft_calls_validate_before_device_work(lib):
         _lib.JHTB_ERR_INVALID
     assert lib.jhtb_legendre_synthesis(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
     assert lib.jhtb_legendre_adjoint(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
+
+
+@pytest.mark.parametrize("nside", [2, 16, 128, 256, 512])
+def test_product_ring_weights_make_m0_quadrature_exact(nside):
+    """jht's weight gates (tests/test_weights.py:40-99): with the product's ring weights the
+    m = 0 quadrature integrates every Legendre polynomial up to degree 2 nside to within
+    1e-9 * 4 pi, the weights sum to 4 pi, and southern rings carry their north partner's
+    weight."""
+    from numpy.polynomial.legendre import legvander
+
+    geo = healpix.RingInfo(nside)
+    pw = weights.pixel_weights(nside)
+    ring_w = np.add.reduceat(pw, geo.startpix)
+    q = ring_w @ legvander(geo.z, 2 * nside)
+    assert abs(q[0] - 4 * np.pi) < 1e-9 * 4 * np.pi
+    assert np.max(np.abs(q[1:])) < 1e-9 * 4 * np.pi
+    assert abs(pw.sum() - 4 * np.pi) < 1e-10
+    per_ring = ring_w / geo.npix_ring
+    np.testing.assert_array_equal(per_ring[: 2 * nside - 1], per_ring[::-1][: 2 * nside - 1])
