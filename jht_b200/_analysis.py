@@ -4,9 +4,10 @@ Drop-in for jht's ``_analysis`` module (src/jht/_analysis.py:49-67):
 ``A0 = S^T W`` and ``niter`` Jacobi steps ``a += A0 (m - S a)``.  The weighted
 residual ``W (m - S a)`` runs as one FP64 kernel (``jhtb_weighted_residual``).
 
-``precision`` (extension) selects the arithmetic of the A0 applications; the
-residual synthesis ``S a`` is always FP64, so the Jacobi fixed point is the FP64
-one and mixed precision only changes how fast it is reached.
+``precision`` (extension) selects the plan of the A0 applications; the residual
+synthesis ``S a`` is always FP64, so the Jacobi fixed point is the FP64 one.  The
+library's adjoint is FP64 in every precision (the tensor-core form covers the
+synthesis only), so ``precision="bf16x3"`` gives the FP64 result here.
 """
 
 from __future__ import annotations
