@@ -275,3 +275,32 @@ def test_oracle_wiener_matches_golden(golden, spin):
         out = O.wiener(golden["wiener/s2_data"], (cl[0], cl[1]), 8, 12, 2, inv_noise=golden["wiener/s2_invn"], tol=1e-10)
         ref = golden["wiener/s2_alm"]
     assert relerr(out, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_oracle_cg_matches_dense_solve(spin):
+    """jht tests/test_masked.py's dense-operator gate: the CG solution of the masked normal
+    equations equals the dense solve of the same system (real-DOF matrix assembled column by
+    column from the oracle's S and S^T)."""
+    nside, lmax, reg = 4, 6, 1e-6
+    rng = np.random.default_rng(20 + spin)
+    geo = O.Rings(nside)
+    zpix = np.repeat(geo.z, geo.nring)
+    mask = (np.abs(zpix) >= 0.3).astype(np.float64)
+    w = mask * O.pixel_weights(nside)
+    w = w if spin == 0 else w[None, :]
+    n = O.n_dof(lmax, spin)
+
+    def normal(x):
+        a = O.real_to_alm(x, lmax, spin)
+        return O.alm_to_real(O.adjoint_synthesis(w * O.synthesis(a, nside, lmax, spin), nside, lmax, spin), lmax, spin)
+
+    A = np.stack([normal(e) for e in np.eye(n)], axis=1) + reg * np.eye(n)
+    assert np.allclose(A, A.T, atol=1e-12)  # the normal operator is symmetric
+    npix = 12 * nside * nside
+    maps = rng.standard_normal(npix) if spin == 0 else rng.standard_normal((2, npix))
+    b = O.alm_to_real(O.adjoint_synthesis(w * maps, nside, lmax, spin), lmax, spin)
+    x_dense = np.linalg.solve(A, b)
+    x_cg = O.alm_to_real(O.deconvolve(maps, mask, nside, lmax, spin, tol=1e-12, reg=reg, max_iter=5000), lmax, spin)
+    assert np.max(np.abs(x_cg - x_dense)) <= 1e-6 * np.max(np.abs(x_dense))
+    assert np.linalg.norm(A @ x_cg - b) <= 1e-10 * np.linalg.norm(b)
