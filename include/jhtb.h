@@ -51,7 +51,7 @@ extern "C" {
 #define JHTB_PREC_FP32 1 /* FP32 contraction, FP32 accumulation (not available yet) */
 #define JHTB_PREC_BF16X3 2 /* batched: mu and a_lm rounded to FP32 and split into three BF16
                               parts; six split products per tile on the tensor cores (tcgen05),
-                              FP32 accumulation folded into FP64 every 64 l */
+                              FP32 accumulation folded into FP64 every 256 l */
 
 typedef struct jhtb_plan jhtb_plan;
 
@@ -154,7 +154,9 @@ int jhtb_dot(const jhtb_plan *plan, int64_t n, const double *x, const double *y,
  * limits it to nside <= 64, lmax <= 1023 and (4 nside - 1)(lmax + 1) <= 131072
  * (larger sizes are rejected with JHTB_ERR_INVALID).  All calls share that array:
  * calls that overlap on the GPU race, so order them on one stream.  The first call
- * on each device looks up the array's address; make it before any stream capture. */
+ * on each device looks up the array's address (and looks it up again when the device's
+ * CUDA context has changed, e.g. after cudaDeviceReset); make it before any stream
+ * capture. */
 int jhtb_synthesis_noalloc(int nside, int lmax, const void *alm, void *map, void *stream);
 
 /* ---- 2D NUFFT stages of the off-grid transforms (_nufft.py:150-191) ----
@@ -224,6 +226,19 @@ int jhtb_plan_timings(jhtb_plan *plan, double *ms, int64_t *counts, int reset);
 /* Device-side error status of the plan's kernels (0 = none, 1 = a bounded wait in a
  * tensor-core kernel timed out).  Synchronises the device to read it; resets it. */
 int jhtb_plan_status(jhtb_plan *plan, int *device_error);
+
+/* Time limit of every bounded wait inside the tensor-core kernels (mbarrier hand-offs
+ * between their warp roles), in nanoseconds, 1e6 .. 6e10; default 2e9.  A wait that runs
+ * out makes the kernel record status 1 (jhtb_plan_status), leave its loops, wait for its
+ * own tensor-core operations in flight and release its tensor memory: the call's output
+ * is then undefined but the context stays usable. */
+int jhtb_plan_set_watchdog(jhtb_plan *plan, int64_t timeout_ns);
+
+/* Fault injection for tests of that failure path (no GPU fault is raised).
+ * JHTB_FAULT_STALL: the tensor-core kernels' operand builders publish nothing, so the
+ * waits on them run out after the watchdog limit.  0 switches injection off. */
+#define JHTB_FAULT_STALL 1
+int jhtb_plan_inject_fault(jhtb_plan *plan, int kind);
 
 /* FP64 FMA throughput probe: a grid of 148*blocks_per_sm CTAs x 256 threads, each
  * running 8 independent FMA chains for `iters` steps.  Writes the elapsed time of

@@ -43,6 +43,8 @@ EXPORTS = (
     "jhtb_probe_fp64_fma",
     "jhtb_synthesis_noalloc",
     "jhtb_plan_status",
+    "jhtb_plan_set_watchdog",
+    "jhtb_plan_inject_fault",
     "jhtb_plan_ring_costs",
     "jhtb_plan_set_ring_range",
     "jhtb_plan_create_rings",
@@ -104,6 +106,8 @@ def load_library(path: str | os.PathLike | None = None):
                                          ctypes.POINTER(ctypes.c_double), vp]),
             "jhtb_synthesis_noalloc": (i32, [i32, i32, vp, vp, vp]),
             "jhtb_plan_status": (i32, [vp, ctypes.POINTER(i32)]),
+            "jhtb_plan_set_watchdog": (i32, [vp, i64]),
+            "jhtb_plan_inject_fault": (i32, [vp, i32]),
             "jhtb_plan_ring_costs": (i32, [vp, i32, ctypes.POINTER(i64), i32]),
             "jhtb_plan_set_ring_range": (i32, [vp, i32, i32]),
             "jhtb_plan_create_rings": (i32, [i32, i32, i32, i32, i32, ctypes.POINTER(HostTables),
@@ -238,6 +242,14 @@ class Plan:
         e = ctypes.c_int()
         check(self.lib.jhtb_plan_status(self.handle, ctypes.byref(e)), "jhtb_plan_status")
         return int(e.value)
+
+    def set_watchdog(self, timeout_ns: int) -> None:
+        """Time limit (ns) of the tensor-core kernels' bounded waits (default 2 s)."""
+        check(self.lib.jhtb_plan_set_watchdog(self.handle, int(timeout_ns)), "jhtb_plan_set_watchdog")
+
+    def inject_fault(self, kind: int) -> None:
+        """Test hook: 1 makes the tensor-core kernels' waits run out (see jhtb.h); 0 turns it off."""
+        check(self.lib.jhtb_plan_inject_fault(self.handle, int(kind)), "jhtb_plan_inject_fault")
 
     def ring_costs(self, granule: int = 256) -> np.ndarray:
         """Legendre work (ring-recursion steps) of each group of `granule` half-grid rings."""

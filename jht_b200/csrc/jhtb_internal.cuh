@@ -145,6 +145,8 @@ struct Plan {
     int *d_tc_order;
     bool tc_owns_tables;
     int *d_err;           // device error flag
+    unsigned long long tc_wait_ns = 2000000000ull;  // time limit of the tensor-core kernels' waits
+    int inject = 0;       // fault injection for tests (kInjectStall)
 
     // ring-pair range of the plan (sharding over devices): half-grid rings
     // [ring_t0, ring_t1) and their southern mirrors; the whole grid by default
@@ -171,6 +173,10 @@ struct Plan {
     };
     std::vector<StageEvent> events;
 };
+
+// Fault injection (tests of the failure path; no GPU fault is raised): the tensor-core
+// kernels' builder warps publish no operand stage, so the waits on them run out.
+constexpr int kInjectStall = JHTB_FAULT_STALL;
 
 enum Stage : int { kStageLegSynth = 0, kStageRingSynth = 1, kStageRingAdj = 2, kStageLegAdj = 3, kNumStages = 4 };
 

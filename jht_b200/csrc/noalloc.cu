@@ -18,12 +18,16 @@
 // streams without ordering, or several host threads) race on it: order them.
 //
 // Set-up: the first call on each device looks up the array's device address with
-// cudaGetSymbolAddress (with that device current) and caches it; make that first
-// call before any stream capture begins.
+// cudaGetSymbolAddress (with that device current) and caches it together with the id
+// of the CUDA context it belongs to; make that first call before any stream capture
+// begins.  When the context changes (cudaDeviceReset destroys the primary context and
+// a later runtime call creates a new one, in which the array may sit elsewhere), the
+// next call sees a different context id and looks the address up again.
 #include <cuda_runtime.h>
 
 #include <atomic>
 #include <cmath>
+#include <mutex>
 
 #include "jhtb_internal.cuh"
 
@@ -38,7 +42,38 @@ constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) double2 g_noalloc_scratch[kNoallocScratchBytes / sizeof(double2)];
 
-std::atomic<double2 *> g_scratch_ptr[kMaxDevices];
+// Per device: the array's address and the id of the context it was looked up in.
+struct ScratchSlot {
+    std::mutex mu;
+    double2 *ptr = nullptr;
+    unsigned long long ctx = 0;
+};
+ScratchSlot g_slot[kMaxDevices];
+
+// Id of the calling thread's current CUDA context (0 if none or if the driver lacks the
+// query), through the driver entry points the runtime hands out (no link-time libcuda).
+unsigned long long current_context_id() {
+    typedef int (*GetCurrentFn)(void **);
+    typedef int (*GetIdFn)(void *, unsigned long long *);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void **)&get_current, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", (void **)&get_id, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+    });
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 // z = cos(theta) of half-grid ring t (0-based), as RING geometry defines it.
 __device__ double ring_z(int t, int nside) {
@@ -63,11 +98,19 @@ __device__ long long ring_start(int r, int nside) {
     return 12LL * nside * nside - 2 * j * (j + 1);
 }
 
-__device__ double ring_phi0(int r, int nside) {
+// phi0 of ring r as pi * p / q with p in {0, 1}: returns q, and p through *p.
+__device__ long long ring_phi0_den(int r, int nside, int *p) {
     const long long i = r + 1;
-    if (i < nside) return M_PI / (4.0 * (double)i);
-    if (i > 3LL * nside) return M_PI / (4.0 * (double)(4LL * nside - i));
-    return ((i - nside) % 2 == 0) ? M_PI / (4.0 * (double)nside) : 0.0;
+    *p = 1;
+    if (i < nside) return 4 * i;
+    if (i > 3LL * nside) return 4 * (4LL * nside - i);
+    *p = ((i - nside) % 2 == 0) ? 1 : 0;
+    return 4LL * nside;
+}
+
+// e^{i m phi0} with the angle reduced exactly: m phi0 / pi = (p m mod 2q) / q.
+__device__ void ring_phase(long long m, int p, long long q, double *s, double *c) {
+    sincospi((double)((p * m) % (2 * q)) / (double)q, s, c);
 }
 
 // One CTA per order m: normalised three-term recursion with scaled seeds
@@ -154,13 +197,14 @@ __global__ void __launch_bounds__(kNoallocThreads) noalloc_ring_kernel(int nside
     __shared__ double2 s_D[4 * kNoallocMaxNside];
     const int r = blockIdx.x;
     const int N = (int)ring_len(r, nside);
-    const double phi0 = ring_phi0(r, nside);
+    int pn = 0;
+    const long long qd = ring_phi0_den(r, nside, &pn);
     const double2 *row = F + (size_t)r * (lmax + 1);
     for (int k = threadIdx.x; k < N; k += blockDim.x) {
         double2 d = make_double2(0.0, 0.0);
         for (int m = k; m <= lmax; m += N) {
             double s, c;
-            sincos((double)m * phi0, &s, &c);
+            ring_phase(m, pn, qd, &s, &c);
             const double2 f = row[m];
             d.x += f.x * c - f.y * s;
             d.y += f.x * s + f.y * c;
@@ -169,7 +213,7 @@ __global__ void __launch_bounds__(kNoallocThreads) noalloc_ring_kernel(int nside
         if (m0 == 0) m0 = N;
         for (int m = m0; m <= lmax; m += N) {
             double s, c;
-            sincos((double)m * phi0, &s, &c);
+            ring_phase(m, pn, qd, &s, &c);
             const double2 f = row[m];
             d.x += f.x * c - f.y * s;
             d.y -= f.x * s + f.y * c;
@@ -207,11 +251,18 @@ extern "C" int jhtb_synthesis_noalloc(int nside, int lmax, const void *alm, void
     int dev = 0;
     JHTB_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(JHTB_ERR_UNSUPPORTED, "jhtb_synthesis_noalloc: device index too large");
-    double2 *scratch = g_scratch_ptr[dev].load();
-    if (!scratch) {
-        // one-time set-up on this device (the device is current): the array's device address
-        JHTB_CUDA_TRY(cudaGetSymbolAddress((void **)&scratch, g_noalloc_scratch));
-        g_scratch_ptr[dev].store(scratch);
+    double2 *scratch = nullptr;
+    {
+        ScratchSlot &slot = g_slot[dev];
+        std::lock_guard<std::mutex> lock(slot.mu);
+        const unsigned long long ctx = current_context_id();
+        if (!slot.ptr || ctx == 0 || ctx != slot.ctx) {
+            // set-up on this device and context (the device is current): the array's device
+            // address; the lookup also creates the primary context if there is none yet
+            JHTB_CUDA_TRY(cudaGetSymbolAddress((void **)&slot.ptr, g_noalloc_scratch));
+            slot.ctx = current_context_id();
+        }
+        scratch = slot.ptr;
     }
     cudaStream_t s = (cudaStream_t)stream;
     noalloc_legendre_kernel<<<lmax + 1, kNoallocThreads, 0, s>>>(nside, lmax, (const double2 *)alm, scratch);

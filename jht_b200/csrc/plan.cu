@@ -263,40 +263,42 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     // (-1)^m sqrt((2l+1)/4pi) for spin 2).  Writing y_l = g_l mu_l with g_lmin = g_lmin+1 = 1,
     // g_l = R_l g_{l-2}, gives mu_l = (alpha_l x + gamma_l) mu_{l-1} - mu_{l-2} and
     // lambda_l = c_l mu_l, c_l = f_l g_l.  alpha = gamma = 0 at l = lmin (the seed step).
+    // The tables are computed in long double (64-bit significand) and rounded once: the
+    // running product g_l would otherwise carry ~sqrt(l) FP64 roundings into c_l, and at
+    // degree 4096 that is a visible part of the transform's error near the poles.
     const long long K = p->K;
     std::vector<double> alpha(K, 0.0), gamma(spin ? K : 0, 0.0), cnorm(K, 0.0);
+    typedef long double xr;
+    const xr kPi = 3.14159265358979323846264338327950288L;
     for (int m = 0; m <= L; ++m) {
         const int lmin = seeds[m].lmin;
-        double g2 = 1.0, g1 = 1.0;  // g_{l-2}, g_{l-1}
-        const double fsign = (spin && (m % 2)) ? -1.0 : 1.0;
+        xr g2 = 1.0L, g1 = 1.0L;  // g_{l-2}, g_{l-1}
+        const xr fsign = (spin && (m % 2)) ? -1.0L : 1.0L;
         for (int l = lmin; l <= L; ++l) {
             const long long idx = alm_index(l, m, L);
-            double P = 0, Q = 0, R = 0;
+            xr P = 0, Q = 0, R = 0;
             if (l > lmin) {
                 if (spin == 0) {
-                    double dl = l;
-                    P = std::sqrt((2 * dl - 1) * (2 * dl + 1) / ((dl - m) * (dl + m)));
-                    R = std::sqrt((2 * dl + 1) * ((dl - 1) * (dl - 1) - (double)m * m) /
-                                  ((2 * dl - 3) * (dl - m) * (dl + m)));
+                    const xr dl = l;
+                    P = sqrtl((2 * dl - 1) * (2 * dl + 1) / ((dl - m) * (dl + m)));
+                    R = sqrtl((2 * dl + 1) * ((dl - 1) * (dl - 1) - (xr)m * m) / ((2 * dl - 3) * (dl - m) * (dl + m)));
                 } else {
                     // Wigner-d coefficients at l-1 producing d^l (_recursion.py:136-143)
-                    double Lp = l - 1, Mm = -m, Mp = 2;
-                    double D = Lp * std::sqrt(((Lp + 1) * (Lp + 1) - Mm * Mm) * ((Lp + 1) * (Lp + 1) - Mp * Mp));
+                    const xr Lp = l - 1, Mm = -m, Mp = 2;
+                    const xr D = Lp * sqrtl(((Lp + 1) * (Lp + 1) - Mm * Mm) * ((Lp + 1) * (Lp + 1) - Mp * Mp));
                     P = (2 * Lp + 1) * Lp * (Lp + 1) / D;
                     Q = -(2 * Lp + 1) * Mm * Mp / D;
-                    R = (Lp + 1) * std::sqrt((Lp * Lp - Mm * Mm) * (Lp * Lp - Mp * Mp)) / D;
+                    R = (Lp + 1) * sqrtl((Lp * Lp - Mm * Mm) * (Lp * Lp - Mp * Mp)) / D;
                 }
             }
-            double g;
-            if (l <= lmin + 1) g = 1.0;
-            else g = R * g2;
+            const xr g = (l <= lmin + 1) ? 1.0L : R * g2;
             if (l > lmin) {
-                alpha[idx] = P * g1 / g;
-                if (spin) gamma[idx] = Q * g1 / g;
+                alpha[idx] = (double)(P * g1 / g);
+                if (spin) gamma[idx] = (double)(Q * g1 / g);
             }
-            const double f = spin ? fsign * std::sqrt((2.0 * l + 1.0) / (4.0 * M_PI)) : 1.0;
-            cnorm[idx] = f * g;
-            if (l > lmin) { g2 = g1; g1 = g; } else { g2 = 1.0; g1 = 1.0; }
+            const xr f = spin ? fsign * sqrtl((2.0L * l + 1.0L) / (4.0L * kPi)) : 1.0L;
+            cnorm[idx] = (double)(f * g);
+            if (l > lmin) { g2 = g1; g1 = g; } else { g2 = 1.0L; g1 = 1.0L; }
         }
     }
     if ((rc = upload(&p->d_alpha, alpha, bytes))) return rc;
@@ -695,6 +697,22 @@ int jhtb_plan_status(jhtb_plan *plan, int *device_error) {
     JHTB_CUDA_TRY(cudaDeviceSynchronize());
     JHTB_CUDA_TRY(cudaMemcpy(device_error, p.d_err, sizeof(int), cudaMemcpyDeviceToHost));
     JHTB_CUDA_TRY(cudaMemset(p.d_err, 0, sizeof(int)));
+    return JHTB_OK;
+}
+
+int jhtb_plan_set_watchdog(jhtb_plan *plan, int64_t timeout_ns) {
+    if (!plan) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_watchdog: NULL plan");
+    if (timeout_ns < 1000000 || timeout_ns > 60000000000LL)
+        return fail(JHTB_ERR_INVALID, "jhtb_plan_set_watchdog: timeout_ns must be in [1e6, 6e10]");
+    reinterpret_cast<Plan *>(plan)->tc_wait_ns = (unsigned long long)timeout_ns;
+    return JHTB_OK;
+}
+
+int jhtb_plan_inject_fault(jhtb_plan *plan, int kind) {
+    if (!plan) return fail(JHTB_ERR_INVALID, "jhtb_plan_inject_fault: NULL plan");
+    if (kind != 0 && kind != JHTB_FAULT_STALL)
+        return fail(JHTB_ERR_INVALID, "jhtb_plan_inject_fault: kind must be 0 or JHTB_FAULT_STALL");
+    reinterpret_cast<Plan *>(plan)->inject = kind;
     return JHTB_OK;
 }
 

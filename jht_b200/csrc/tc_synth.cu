@@ -34,6 +34,7 @@
 #include <algorithm>
 
 #include "jhtb_internal.cuh"
+#include "tc_common.cuh"
 
 namespace jhtb {
 namespace {
@@ -47,149 +48,8 @@ constexpr int kTcK = 16;         // l steps per chunk = MMA K (BF16)
 #define JHTB_TC_NSA 2
 #endif
 constexpr int kFlush = JHTB_TC_FLUSH;  // chunks per FP32 accumulation block (256 l)
-constexpr unsigned kWaitLimit = 1u << 26;
 
-// ---------------------------------------------------------------------------------
-// PTX wrappers
-// ---------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(ncols)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_relinquish() {
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t globaltimer_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-// Bounded wait (iteration count and ~2 s of wall time); returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    const uint64_t t0 = globaltimer_ns();
-    for (unsigned it = 0; it < kWaitLimit; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 1023u) == 1023u && globaltimer_ns() - t0 > 2000000000ull) return false;
-    }
-    return false;
-}
-
-// A operand from tensor memory (ts form), B from a shared-memory descriptor.
-__device__ __forceinline__ void umma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
-                                            uint32_t acc) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(
-            d_tmem),
-        "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(acc)
-        : "memory");
-}
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// 32 lanes x 8 consecutive 32-bit columns <-> 8 registers per thread (its own lane's row).
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(a), "r"(b), "r"(c),
-                 "r"(d)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
-
-// Shared-memory descriptor, K-major, no swizzle: 8-row x 16-byte core matrices,
-// LBO = byte distance between the two 8-element K halves, SBO = between 8-row groups.
-__device__ __forceinline__ uint64_t smem_desc(const void *p, uint32_t lbo, uint32_t sbo) {
-    const uint32_t a = smem_u32(p);
-    return (uint64_t)((a >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);  // version 1 (sm100), swizzle none
-}
-
-// kind::f16 instruction descriptor: FP32 accumulate, BF16 A and B, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-// Byte offset of element (row, k) in a K-major no-swizzle tile with LBO 128, SBO 256
-// (K = 16): core matrix (row/8, k/8) at (row/8)*256 + (k/8)*128, row-in-core * 16 + k%8 * 2.
-__device__ __forceinline__ uint32_t kmaj_off(int row, int k) {
-    return (uint32_t)((row >> 3) * 256 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
-}
-
-// x ~ h + m + l with h, m, l BF16: x is rounded to FP32, then each part keeps the top
-// 16 bits of the remaining residual (a truncation, exact in FP32), so h + m + l differs
-// from x by less than 2^-24 |x|.  Returns the three parts as FP32 bit patterns whose
-// low halves are zero (the BF16 value is the high half).
-__device__ __forceinline__ void split3_bits(double xd, uint32_t &h, uint32_t &m, uint32_t &l) {
-    const float x = (float)xd;
-    h = __float_as_uint(x) & 0xFFFF0000u;
-    const float r1 = x - __uint_as_float(h);
-    m = __float_as_uint(r1) & 0xFFFF0000u;
-    const float r2 = r1 - __uint_as_float(m);
-    l = __float_as_uint(r2) & 0xFFFF0000u;
-}
-// BF16 of FP32 value x by truncation (used for the B tiles, same split as split3_bits)
-__device__ __forceinline__ void split3(double xd, __nv_bfloat16 &h, __nv_bfloat16 &m, __nv_bfloat16 &l) {
-    uint32_t hb, mb, lb;
-    split3_bits(xd, hb, mb, lb);
-    h = __ushort_as_bfloat16((unsigned short)(hb >> 16));
-    m = __ushort_as_bfloat16((unsigned short)(mb >> 16));
-    l = __ushort_as_bfloat16((unsigned short)(lb >> 16));
-}
-
-
-__device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {
-    if (sc < 0 && fabs(u) > kBig) {
-        u *= kScaleDown;
-        prev *= kScaleDown;
-        sc += 1;
-    }
-}
-
-// Two values at once, packed as BF16 pairs (x0's part in the low half) from the
-// truncation split of split3_bits; only the FP64 -> FP32 rounding uses the conversion
-// pipe, the rest is integer and FP32 arithmetic.
-__device__ __forceinline__ void split3_pair(double x0d, double x1d, uint32_t &h, uint32_t &m, uint32_t &l) {
-    uint32_t h0, m0, l0, h1, m1, l1;
-    split3_bits(x0d, h0, m0, l0);
-    split3_bits(x1d, h1, m1, l1);
-    h = __byte_perm(h0, h1, 0x7632);
-    m = __byte_perm(m0, m1, 0x7632);
-    l = __byte_perm(l0, l1, 0x7632);
-}
+using namespace tc;
 
 struct TcParams {
     int lmax, T, nrings, M, nside;
@@ -204,6 +64,8 @@ struct TcParams {
     const int *stsc;
     const int *order;
     int *err;
+    unsigned long long wait_ns;  // time limit of every bounded wait
+    int inject;                  // fault injection for tests (kInjectStall: builders publish nothing)
 };
 
 template <int SPIN, int BM>
@@ -272,7 +134,10 @@ __device__ __forceinline__ TcItem tc_item(const TcParams &p, int it, int nitems,
     return tc_item_of(p, it, __ldg(&p.order[it % nitems]), nitems, nb, bm);
 }
 
-__device__ __forceinline__ bool tc_failed(const int *f) { return *(volatile const int *)f != 0; }
+// Whether any role has recorded a failure; one verdict per warp (see mbar_wait_warp).
+__device__ __forceinline__ bool tc_failed(const int *f) {
+    return __any_sync(0xffffffffu, *(volatile const int *)f != 0);
+}
 __device__ __forceinline__ void tc_fail(int *f, int *err) {
     *(volatile int *)f = 1;
     atomicExch(err, 1);
@@ -426,8 +291,8 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
         const int nck = i_start < nst ? (nst - i_start + kTcK - 1) / kTcK : 0;
         for (int c = 0; c < nck; ++c, ++gc) {
             const int sA = gc % C::NSA, sB = gc % C::NSB;
-            if (!mbar_wait(&sm.fullB[sB], (gc / C::NSB) & 1u)) { ok = false; break; }
-            if (gc >= (unsigned)C::NSA && !mbar_wait(&sm.emptyA[sA], ((gc / C::NSA) - 1u) & 1u)) { ok = false; break; }
+            if (!mbar_wait_warp(&sm.fullB[sB], (gc / C::NSB) & 1u, p.wait_ns)) { ok = false; break; }
+            if (gc >= (unsigned)C::NSA && !mbar_wait_warp(&sm.emptyA[sA], ((gc / C::NSA) - 1u) & 1u, p.wait_ns)) { ok = false; break; }
             tc_fence_after();  // the stage's previous MMAs are complete before it is overwritten
             uint32_t tA[CH];
 #pragma unroll
@@ -454,7 +319,7 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
             }
             const bool last = c == nck - 1;
             if ((c % kFlush) == kFlush - 1 || last) {
-                if (!mbar_wait(&sm.accFull, bk & 1u)) { ok = false; break; }
+                if (!mbar_wait_warp(&sm.accFull, bk & 1u, p.wait_ns)) { ok = false; break; }
                 tc_fence_after();
                 const bool first_block = c < kFlush;
                 const int b_lo = (it / nitems) * BM, b_cnt = min(BM, nb - b_lo);
@@ -589,6 +454,8 @@ __device__ void tc_builder(const TcParams &p, const double2 *__restrict__ alm_al
     using C = TcCfg<SPIN, BM>;
     const int k = bt % kTcK, bm = bt / kTcK;
     const double sg = (k & 1) ? -1.0 : 1.0;  // (-1)^(l - lmin): chunks start at even offsets
+    // test hook: no operand stage is ever published, so every wait on one runs out
+    if (p.inject == kInjectStall) return;
     const int nitems = p.norder;
     // the loads run two chunks ahead of the stores
     TcCursor<BM> ld{(int)blockIdx.x, 0, nitems * ((nb + BM - 1) / BM), nitems, nb, TcItem{}};
@@ -602,7 +469,7 @@ __device__ void tc_builder(const TcParams &p, const double2 *__restrict__ alm_al
     while (r0.live) {
         if (tc_failed(&sm.fail)) break;
         const int sB = gc % C::NSB;
-        if (gc >= (unsigned)C::NSB && !mbar_wait(&sm.emptyB[sB], ((gc / C::NSB) - 1u) & 1u)) { ok = false; break; }
+        if (gc >= (unsigned)C::NSB && !mbar_wait_warp(&sm.emptyB[sB], ((gc / C::NSB) - 1u) & 1u, p.wait_ns)) { ok = false; break; }
         double col[C::NBT][4];
         if (SPIN) {
             // cp = -(aE + i aB) c, cm = -(aE - i aB) c   (healpix.py:316-318)
@@ -662,8 +529,8 @@ __device__ void tc_mma(const TcParams &p, TcSmem<SPIN, BM> &sm, int nb, uint32_t
             const int sA = gc % C::NSA, sB = gc % C::NSB;
             const bool bstart = (c % kFlush) == 0;
             const bool bend = (c % kFlush) == kFlush - 1 || c == nck - 1;
-            if (!mbar_wait(&sm.fullA[sA], (gc / C::NSA) & 1u) || !mbar_wait(&sm.fullB[sB], (gc / C::NSB) & 1u) ||
-                (bstart && bk > 0 && !mbar_wait(&sm.accEmpty, (bk - 1u) & 1u))) {
+            if (!mbar_wait_warp(&sm.fullA[sA], (gc / C::NSA) & 1u, p.wait_ns) || !mbar_wait_warp(&sm.fullB[sB], (gc / C::NSB) & 1u, p.wait_ns) ||
+                (bstart && bk > 0 && !mbar_wait_warp(&sm.accEmpty, (bk - 1u) & 1u, p.wait_ns))) {
                 ok = false;
                 break;
             }
@@ -699,7 +566,7 @@ __device__ void tc_mma(const TcParams &p, TcSmem<SPIN, BM> &sm, int nb, uint32_t
     // every issued MMA has completed before tensor memory is released
     if (lane == 0) {
         umma_commit(&sm.fin);
-        if (!mbar_wait(&sm.fin, 0u)) tc_fail(&sm.fail, p.err);
+        if (!mbar_wait(&sm.fin, 0u, p.wait_ns)) tc_fail(&sm.fail, p.err);  // lane 0 alone
     }
     __syncwarp();
 }
@@ -796,6 +663,8 @@ int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaS
     q.order = p.d_tc_order;
     q.norder = p.tc_norder;
     q.err = p.d_err;
+    q.wait_ns = p.tc_wait_ns;
+    q.inject = p.inject;
     // whole groups of kTcMaps maps share one recursion (one CTA per SM, N = 4 kTcMaps);
     // a remainder runs in groups of 8 (two CTAs per SM), so a short batch does not pay
     // for the columns of a full group

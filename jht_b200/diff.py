@@ -55,7 +55,7 @@ def bandpower(alm, lmax: int, spin: int = 0) -> torch.Tensor:
     a = alm if isinstance(alm, torch.Tensor) else torch.as_tensor(np.asarray(alm))
     dev = a.device
     ells = torch.as_tensor(_ell_of_idx(lmax), device=dev)
-    wgt = torch.as_tensor(alm_metric_weight(lmax), device=dev)
+    wgt = torch.as_tensor(np.array(alm_metric_weight(lmax)), device=dev)
     norm = 1.0 / (2.0 * torch.arange(lmax + 1, device=dev, dtype=torch.float64) + 1.0)
 
     def one(v):

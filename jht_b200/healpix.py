@@ -171,7 +171,7 @@ def _m0_mask(lmax: int, device_index: int) -> torch.Tensor:
 
 @lru_cache(maxsize=None)
 def _metric(lmax: int, device_index: int) -> torch.Tensor:
-    return torch.as_tensor(alm_metric_weight(lmax), device=torch.device("cuda", device_index))
+    return torch.as_tensor(np.array(alm_metric_weight(lmax)), device=torch.device("cuda", device_index))
 
 
 def _synthesis_cotangent(b: torch.Tensor, lmax: int, spin: int) -> torch.Tensor:

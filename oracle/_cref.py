@@ -29,13 +29,14 @@ class _Ref:
         self.lib = lib
         argt = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                 ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
-        lib.oracle_synth.argtypes = argt
-        lib.oracle_adjoint.argtypes = argt
-        lib.oracle_synth.restype = None
-        lib.oracle_adjoint.restype = None
+        for name in ("oracle_synth", "oracle_adjoint", "oracle_synth_ld", "oracle_adjoint_ld"):
+            getattr(lib, name).argtypes = argt
+            getattr(lib, name).restype = None
 
-    def synth(self, spin, lmax, x, alm, m_lo=0, m_hi=None):
-        """Half-grid synthesis contraction; alm is (ncomp, K). Returns 2 (spin 0) or 4 (M, T) arrays."""
+    def synth(self, spin, lmax, x, alm, m_lo=0, m_hi=None, extended=False):
+        """Half-grid synthesis contraction; alm is (ncomp, K). Returns 2 (spin 0) or 4 (M, T) arrays.
+
+        ``extended=True`` runs the same algorithm in 80-bit long double (the arbiter)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
         T = x.size
         M = lmax + 1
@@ -43,11 +44,14 @@ class _Ref:
         alm = np.ascontiguousarray(alm, dtype=np.complex128)
         nout = 2 if spin == 0 else 4
         out = np.zeros((nout, M, T), np.complex128)
-        self.lib.oracle_synth(spin, lmax, T, x.ctypes.data, alm.ctypes.data, out.ctypes.data, m_lo, m_hi)
+        f = self.lib.oracle_synth_ld if extended else self.lib.oracle_synth
+        f(spin, lmax, T, x.ctypes.data, alm.ctypes.data, out.ctypes.data, m_lo, m_hi)
         return tuple(out)
 
-    def adjoint(self, spin, lmax, x, V, m_lo=0, m_hi=None):
-        """Half-grid adjoint contraction; V is a list of (M, T). Returns packed (K,) arrays."""
+    def adjoint(self, spin, lmax, x, V, m_lo=0, m_hi=None, extended=False):
+        """Half-grid adjoint contraction; V is a list of (M, T). Returns packed (K,) arrays.
+
+        ``extended=True`` runs the same algorithm in 80-bit long double (the arbiter)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
         T = x.size
         M = lmax + 1
@@ -56,7 +60,8 @@ class _Ref:
         Vin = np.ascontiguousarray(np.stack(V), dtype=np.complex128)
         nout = 1 if spin == 0 else 2
         out = np.zeros((nout, K), np.complex128)
-        self.lib.oracle_adjoint(spin, lmax, T, x.ctypes.data, Vin.ctypes.data, out.ctypes.data, m_lo, m_hi)
+        f = self.lib.oracle_adjoint_ld if extended else self.lib.oracle_adjoint
+        f(spin, lmax, T, x.ctypes.data, Vin.ctypes.data, out.ctypes.data, m_lo, m_hi)
         return tuple(out)
 
 

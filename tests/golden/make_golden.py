@@ -238,4 +238,6 @@ def offgrid_fixtures(jht) -> dict[str, np.ndarray]:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py /path/to/jht/checkout")
+    main(sys.argv[1])

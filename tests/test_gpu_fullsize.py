@@ -1,23 +1,29 @@
-"""Parity at the full benchmark size (nside 2048, lmax 4096, spin 2) on a B200.
+"""Parity at the full benchmark size (nside 2048, lmax 4096) on a B200, against an
+extended-precision arbiter.
 
-The oracle cannot run a whole transform at this size in test time, so these checks
-use properties that do not depend on size:
+Two FP64 evaluations of the degree-4096 recursion -- jht's own log-renormalised form
+(the oracle) and the kernels' scaled normalised form -- both round, and near the poles
+each lands about 1e-12 of the map's maximum away from the exact transform.  Which side
+carries a difference is decided by the arbiter: the oracle's algorithm carried out in
+80-bit long double (``oracle/legendre_ref.c``, ``extended=True``), 2048 times finer than
+FP64.  Every check below measures the CUDA path's error against the arbiter and the
+oracle's error against the arbiter on the same entries, and requires the CUDA path to
+be within 1e-12 of the arbiter or no less accurate than jht's own FP64 algorithm.
 
-* m-sparse synthesis: a_lm non-zero only on a few m columns (low, middle and the
-  last ones, where the recursion starts deepest into the underflow region near the
-  poles); the map is compared on sampled rings (poles, caps, belt, equator) with a
-  direct evaluation of the oracle's per-ring Fourier series;
-* m-subset adjoint: the GPU S^T of a full random map, compared on the same m
-  columns with the oracle's contraction of the per-ring DFTs;
-* the inner-product identity <S a, v> = <a, S^T v>_G on the whole band.
+* full-band synthesis: the seeded benchmark input (all l, m) on 46 sampled rings
+  (both poles, caps, belt, equator), the Legendre stage evaluated by the arbiter at
+  those rings only;
+* full-band adjoint: a map that is non-zero on the same sampled rings, all a_lm;
+* m-subset adjoint of a full random map (every ring contributes) on m columns at the
+  low, middle and high end;
+* the inner-product identity <S a, v> = <a, S^T v>_G on the whole band, and the VJP
+  against central differences on 64 real-DOF directions.
 """
 
 from __future__ import annotations
 
 import numpy as np
 import pytest
-
-from conftest import relerr
 
 pytestmark = [pytest.mark.gpu, pytest.mark.slow]
 
@@ -30,134 +36,187 @@ from oracle import _cref  # noqa: E402
 from oracle import jht_oracle as O  # noqa: E402
 
 NSIDE, LMAX = 2048, 4096
+T = 2 * NSIDE
 M_RANGES = [(0, 4), (1501, 1505), (4090, 4097)]
-# Two FP64 evaluations of the degree-4096 three-term recursion (the oracle's
-# log-renormalised form and the kernels' scaled form) each carry rounding of up to
-# ~1e-10 of the amplitude sqrt((2l+1)/4pi) on the polar rings (x -> 1), measured
-# against an 80-bit evaluation of the same recursion; over a map that leaves a few
-# 1e-12.  The reference reports 2.5e-11 .. 6.5e-11 between its own FP64 synthesis
-# and ducc0 at nside 2048, lmax 2000..3000 (docs/accuracy.md:139-149).
-TOL = 2e-11
+# Accept the CUDA path if it is within ABS_TOL of the arbiter, or no further from it
+# than the FP64 oracle is (the slack allows for the two roundings being independent
+# draws of the same size).
+ABS_TOL = 1e-12
+SLACK = 1.1
 
 
-def _sampled_rings(nside):
-    nr = 4 * nside - 1
-    picks = {0, 1, 2, 5, nside // 2, nside - 1, nside, nside + 1, 2 * nside - 2, 2 * nside - 1, 2 * nside,
-             3 * nside - 1, 3 * nside, nr - 3, nr - 2, nr - 1}
-    return sorted(r for r in picks if 0 <= r < nr)
+def _half_rings():
+    """Sampled half-grid rings: the polar ones, a geometric spread, the equator region."""
+    t = np.concatenate([np.arange(8), np.geomspace(8, T - 1, 12).astype(int), [NSIDE - 1, NSIDE, T - 2, T - 1]])
+    return np.unique(t)
 
 
-def _m_sparse_alm(rng, spin):
-    K = O.alm_size(LMAX)
-    a = np.zeros((2, K), np.complex128) if spin == 2 else np.zeros((1, K), np.complex128)
-    for lo, hi in M_RANGES:
-        for m in range(lo, hi):
-            b = O.alm_base(m, LMAX)
-            n = LMAX + 1 - m
-            ell = np.arange(m, LMAX + 1)
-            v = (rng.standard_normal((a.shape[0], n)) + 1j * rng.standard_normal((a.shape[0], n))) / (ell + 10.0)
-            if m == 0:
-                v = v.real.astype(np.complex128)
-            if spin == 2:
-                v[:, ell < 2] = 0
-            a[:, b : b + n] = v
-    return a
+def _full_rings(half):
+    out = []
+    for t in half:
+        out.append(int(t))
+        if t < T - 1:
+            out.append(4 * NSIDE - 2 - int(t))
+    return sorted(out)
 
 
-def _ring_F(F_north, F_south, geo, r):
-    """Column of the full (M, nrings) coefficient matrix for ring r (the (-1)^m mirror below the equator)."""
-    T = 2 * geo.nside
-    if r < T:
-        return F_north[:, r]
-    t = 4 * geo.nside - 2 - r
-    return ((-1.0) ** np.arange(F_north.shape[0])) * F_south[:, t]
+def _config_alm(spin):
+    """The benchmark's seeded input: E with C_l = 1/(l+10)^2, B 0.1/(l+10)^2, l < 2 zero."""
+    rng = np.random.default_rng(1234)
+    ell, _ = O.lm_of_index(LMAX)
+    out = []
+    for amp in (1.0, 0.1):
+        cl = amp / (ell + 10.0) ** 2
+        g1, g2 = rng.standard_normal(ell.size), rng.standard_normal(ell.size)
+        a = np.sqrt(cl / 2.0) * (g1 + 1j * g2)
+        a[: LMAX + 1] = np.sqrt(cl[: LMAX + 1]) * g1[: LMAX + 1]
+        if spin == 2:
+            a[ell < 2] = 0.0
+        out.append(a)
+    return np.stack(out) if spin == 2 else out[0][None, :]
 
 
-def _eval_ring(Gp, Gm, N):
-    """value_j = sum_m Gp[m] e^{2 pi i m j / N} + sum_{m>=1} conj(Gm[m]) e^{-2 pi i m j / N} on the sparse m set."""
-    j = np.arange(N)
-    out = np.zeros(N, np.complex128)
-    for lo, hi in M_RANGES:
-        for m in range(lo, hi):
-            e = np.exp(2j * np.pi * ((m * j) % N) / N)
-            out += Gp[m] * e
-            if m >= 1:
-                out += np.conj(Gm[m]) * np.conj(e)
-    return out
+def _ring_samples(parts, col, geo, r, spin):
+    """RING samples of ring r from half-grid Legendre sums (oracle layout) at column col[t]."""
+    m = np.arange(LMAX + 1)
+    north = r < T
+    c = col[r if north else 4 * NSIDE - 2 - r]
+    sgn = 1.0 if north else (-1.0) ** m
+    ph = np.exp(1j * m * geo.phi0[r])
+    if spin == 0:
+        Gp = Gm = sgn * (parts[0][:, c] if north else parts[1][:, c]) * ph
+    else:
+        Gp = sgn * (parts[0][:, c] if north else parts[1][:, c]) * ph
+        Gm = sgn * (parts[2][:, c] if north else parts[3][:, c]) * ph
+    N = int(geo.nring[r])
+    D = np.zeros(N, np.complex128)
+    np.add.at(D, m % N, Gp)
+    np.add.at(D, (-m[1:]) % N, np.conj(Gm[1:]))
+    y = np.fft.ifft(D) * N
+    return y.real[None, :] if spin == 0 else np.stack([y.real, y.imag])
+
+
+def _errors(got, fp64, arb):
+    den = max(float(np.max(np.abs(arb))), 1e-300)
+    return float(np.max(np.abs(got - arb))) / den, float(np.max(np.abs(fp64 - arb))) / den
+
+
+def _check(name, e_gpu, e_orc):
+    print(f"{name}: CUDA vs arbiter {e_gpu:.3e}, jht FP64 algorithm vs arbiter {e_orc:.3e}")
+    assert e_gpu <= max(ABS_TOL, SLACK * e_orc), (name, e_gpu, e_orc)
 
 
 @pytest.mark.parametrize("spin", [2, 0])
-def test_m_sparse_synthesis_full_size(spin):
-    rng = np.random.default_rng(100 + spin)
-    a = _m_sparse_alm(rng, spin)
+def test_full_band_synthesis_vs_arbiter(spin):
     geo = O.Rings(NSIDE)
-    x = geo.z[: 2 * NSIDE]
+    half = _half_rings()
+    col = {int(t): k for k, t in enumerate(half)}
+    x = geo.z[half]
+    a = _config_alm(spin)
     ref = _cref.load()
-    parts = None
-    for lo, hi in M_RANGES:
-        out = ref.synth(spin, LMAX, x, a, lo, hi)
-        parts = list(out) if parts is None else [p + o for p, o in zip(parts, out)]
-    got = jhtb.synthesis(a[0] if spin == 0 else a, NSIDE, LMAX, spin).cpu().numpy()
-    got = got.reshape(-1, geo.npix)
-    worst, scale = 0.0, 0.0
-    for r in _sampled_rings(NSIDE):
+    arb = ref.synth(spin, LMAX, x, a, extended=True)
+    f64 = ref.synth(spin, LMAX, x, a)
+    got = jhtb.synthesis(a[0] if spin == 0 else a, NSIDE, LMAX, spin).cpu().numpy().reshape(-1, geo.npix)
+    G, E, F = [], [], []
+    for r in _full_rings(half):
+        s, N = int(geo.start[r]), int(geo.nring[r])
+        G.append(got[:, s : s + N])
+        E.append(_ring_samples(arb, col, geo, r, spin))
+        F.append(_ring_samples(f64, col, geo, r, spin))
+    e_gpu, e_orc = _errors(np.concatenate(G, 1), np.concatenate(F, 1), np.concatenate(E, 1))
+    _check(f"synthesis spin {spin}", e_gpu, e_orc)
+
+
+def _ring_inputs(d, geo, rings, col, ncol, spin):
+    """Half-grid adjoint inputs (oracle layout) of the rings' forward DFTs."""
+    M = LMAX + 1
+    m = np.arange(M)
+    z = d[0] if spin == 0 else d[0] + 1j * d[1]
+    V = [np.zeros((M, ncol), np.complex128) for _ in range(2 if spin == 0 else 4)]
+    for r in rings:
         N, s = int(geo.nring[r]), int(geo.start[r])
-        ph = np.exp(1j * np.arange(LMAX + 1) * geo.phi0[r])
-        if spin == 0:
-            F = _ring_F(parts[0], parts[1], geo, r) * ph
-            val = _eval_ring(F, F, N).real
-            exp = val[None, :]
+        W = np.fft.fft(z[s : s + N].astype(np.complex128))
+        ph = np.exp(-1j * m * geo.phi0[r])
+        wp = W[m % N] * ph
+        wm = np.conj(W[(-m) % N]) * ph
+        if r < T:
+            c = col[r]
+            V[0][:, c] = wp
+            if spin == 2:
+                V[2][:, c] = wm
         else:
-            Fp = _ring_F(parts[0], parts[1], geo, r) * ph
-            Fm = _ring_F(parts[2], parts[3], geo, r) * ph
-            val = _eval_ring(Fp, Fm, N)
-            exp = np.stack([val.real, val.imag])
-        worst = max(worst, float(np.max(np.abs(got[:, s : s + N] - exp))))
-        scale = max(scale, float(np.max(np.abs(exp))))
-    assert scale > 0
-    assert worst / scale <= TOL
+            c = col[4 * NSIDE - 2 - r]
+            sg = (-1.0) ** m
+            V[1][:, c] = sg * wp
+            if spin == 2:
+                V[3][:, c] = sg * wm
+    return V
 
 
-def test_m_subset_adjoint_full_size():
+def _alm_from_parts(parts, spin):
+    if spin == 0:
+        return parts[0][None, :]
+    p2, m2 = parts
+    return np.stack([0.5 * (-p2 - m2), 0.5 * (1j * p2 - 1j * m2)])
+
+
+@pytest.mark.parametrize("spin", [2, 0])
+def test_full_band_adjoint_vs_arbiter(spin):
+    """S^T of a map that is non-zero on the sampled rings only: every (l, m) is exercised."""
+    geo = O.Rings(NSIDE)
+    half = _half_rings()
+    col = {int(t): k for k, t in enumerate(half)}
+    rings = _full_rings(half)
+    rng = np.random.default_rng(77 + spin)
+    d = np.zeros((1 if spin == 0 else 2, geo.npix))
+    for r in rings:
+        s, N = int(geo.start[r]), int(geo.nring[r])
+        d[:, s : s + N] = rng.standard_normal((d.shape[0], N))
+    V = _ring_inputs(d, geo, rings, col, len(half), spin)
+    ref = _cref.load()
+    x = geo.z[half]
+    arb = _alm_from_parts(ref.adjoint(spin, LMAX, x, V, extended=True), spin)
+    f64 = _alm_from_parts(ref.adjoint(spin, LMAX, x, V), spin)
+    got = jhtb.adjoint_synthesis(d[0] if spin == 0 else d, NSIDE, LMAX, spin).cpu().numpy().reshape(arb.shape)
+    e_gpu, e_orc = _errors(got, f64, arb)
+    _check(f"adjoint spin {spin}", e_gpu, e_orc)
+
+
+def test_m_subset_adjoint_vs_arbiter():
+    """S^T of a full random map on the m columns of M_RANGES: all 4096 rings contribute."""
     spin = 2
     rng = np.random.default_rng(7)
     geo = O.Rings(NSIDE)
-    T = 2 * NSIDE
-    x = geo.z[:T]
     d = rng.standard_normal((2, geo.npix))
     got = jhtb.adjoint_synthesis(d, NSIDE, LMAX, spin).cpu().numpy()
-    M = LMAX + 1
     ms = np.concatenate([np.arange(lo, hi) for lo, hi in M_RANGES])
-    Vpn = np.zeros((M, T), np.complex128)
-    Vmn = np.zeros((M, T), np.complex128)
-    Sp = np.zeros((M, T), np.complex128)
-    Sm = np.zeros((M, T), np.complex128)
+    M = LMAX + 1
+    V = [np.zeros((M, T), np.complex128) for _ in range(4)]
     z = d[0] + 1j * d[1]
     sign = (-1.0) ** ms
     for N in np.unique(geo.nring):
         rows = np.flatnonzero(geo.nring == N)
         pix = geo.start[rows][:, None] + np.arange(N)[None, :]
         W = np.fft.fft(z[pix], axis=1)
-        wp = W[:, ms % N] * np.exp(-1j * ms[None, :] * geo.phi0[rows][:, None])
-        wm = np.conj(W[:, (-ms) % N]) * np.exp(-1j * ms[None, :] * geo.phi0[rows][:, None])
+        ph = np.exp(-1j * ms[None, :] * geo.phi0[rows][:, None])
+        wp, wm = W[:, ms % N] * ph, np.conj(W[:, (-ms) % N]) * ph
         for k, r in enumerate(rows):
             if r < T:
-                Vpn[ms, r] = wp[k]
-                Vmn[ms, r] = wm[k]
+                V[0][ms, r], V[2][ms, r] = wp[k], wm[k]
             else:
                 t = 4 * NSIDE - 2 - r
-                Sp[ms, t] = sign * wp[k]
-                Sm[ms, t] = sign * wm[k]
+                V[1][ms, t], V[3][ms, t] = sign * wp[k], sign * wm[k]
     ref = _cref.load()
-    p2 = np.zeros(O.alm_size(LMAX), np.complex128)
-    m2 = np.zeros_like(p2)
+    x = geo.z[:T]
+    K = O.alm_size(LMAX)
+    arb = np.zeros((2, K), np.complex128)
+    f64 = np.zeros((2, K), np.complex128)
     for lo, hi in M_RANGES:
-        a, b = ref.adjoint(2, LMAX, x, [Vpn, Sp, Vmn, Sm], lo, hi)
-        p2 += a
-        m2 += b
-    exp = np.stack([0.5 * (-p2 - m2), 0.5 * (1j * p2 - 1j * m2)])
+        arb += _alm_from_parts(ref.adjoint(2, LMAX, x, V, lo, hi, extended=True), 2)
+        f64 += _alm_from_parts(ref.adjoint(2, LMAX, x, V, lo, hi), 2)
     idx = np.concatenate([O.alm_base(m, LMAX) + np.arange(LMAX + 1 - m) for m in ms])
-    assert relerr(got[:, idx], exp[:, idx]) <= TOL
+    e_gpu, e_orc = _errors(got[:, idx], f64[:, idx], arb[:, idx])
+    _check("adjoint m-subset, all rings", e_gpu, e_orc)
 
 
 def test_inner_product_identity_full_size():
@@ -172,7 +231,7 @@ def test_inner_product_identity_full_size():
     v = torch.randn((2, 12 * NSIDE * NSIDE), dtype=torch.float64, device="cuda", generator=gen)
     lhs = float(torch.sum(jhtb.synthesis(a, NSIDE, LMAX, spin) * v))
     b = jhtb.adjoint_synthesis(v, NSIDE, LMAX, spin)
-    G = torch.as_tensor(jhtb.alm_metric_weight(LMAX), device="cuda")
+    G = torch.as_tensor(jhtb.alm_metric_weight(LMAX).copy(), device="cuda")
     rhs = float(torch.sum(G * torch.real(torch.conj(a) * b)))
     assert abs(lhs - rhs) <= 1e-11 * abs(lhs)
 

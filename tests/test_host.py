@@ -88,6 +88,8 @@ def test_null_pointers_are_rejected(lib):
     assert lib.jhtb_synthesis(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
     assert lib.jhtb_adjoint_synthesis(None, None, None, 1, None) == _lib.JHTB_ERR_INVALID
     assert lib.jhtb_plan_destroy(None) == _lib.JHTB_OK
+    assert lib.jhtb_plan_set_watchdog(None, 10**9) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_plan_inject_fault(None, 1) == _lib.JHTB_ERR_INVALID
 
 
 @pytest.mark.parametrize("nside", [1, 4, 13, 64])

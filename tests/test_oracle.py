@@ -304,3 +304,85 @@ def test_oracle_cg_matches_dense_solve(spin):
     x_cg = O.alm_to_real(O.deconvolve(maps, mask, nside, lmax, spin, tol=1e-12, reg=reg, max_iter=5000), lmax, spin)
     assert np.max(np.abs(x_cg - x_dense)) <= 1e-6 * np.max(np.abs(x_dense))
     assert np.linalg.norm(A @ x_cg - b) <= 1e-10 * np.linalg.norm(b)
+
+
+# ------------------------------------------------------------------------------------
+# the extended-precision arbiter (oracle/legendre_ref.c in long double) against a
+# 30-digit mpmath evaluation of the same sums: it must be far below FP64 rounding
+# ------------------------------------------------------------------------------------
+def _mp_column_sum(spin, m, lmax, x, coef):
+    """sum_l coef[l - lmin] lambda^{s}_lm(x) (spin 0), or the +2 / -2 sums (spin 2), in mpmath."""
+    import mpmath as mp
+
+    mp.mp.dps = 30
+    xm = mp.mpf(x)
+    th = mp.acos(xm)
+    if spin == 0:
+        c = -mp.mpf(0.5) * mp.log(4 * mp.pi)
+        for k in range(1, m + 1):
+            c += mp.mpf(0.5) * mp.log(mp.mpf(2 * k + 1) / (2 * k))
+        cur, prev = (-1) ** m * mp.e**c * mp.sin(th) ** m, mp.mpf(0)
+        tot = mp.mpc(coef[0]) * cur
+        for ell in range(m + 1, lmax + 1):
+            L = mp.mpf(ell)
+            a = mp.sqrt((2 * L - 1) * (2 * L + 1) / ((L - m) * (L + m)))
+            b = mp.sqrt((2 * L + 1) * ((L - 1) ** 2 - m * m) / ((2 * L - 3) * (L - m) * (L + m)))
+            prev, cur = cur, a * xm * cur - b * prev
+            tot += mp.mpc(coef[ell - m]) * cur
+        return [tot]
+    out = []
+    lmin = max(m, 2)
+    for Mp in (2, -2):
+        M = -m
+        k0 = max(0, M - Mp)
+        lf = mp.mpf(0.5) * (mp.loggamma(lmin + M + 1) + mp.loggamma(lmin - M + 1) + mp.loggamma(lmin + Mp + 1)
+                            + mp.loggamma(lmin - Mp + 1)) - (mp.loggamma(k0 + 1) + mp.loggamma(lmin + M - k0 + 1)
+                                                             + mp.loggamma(lmin - Mp - k0 + 1) + mp.loggamma(k0 - M + Mp + 1))
+        cur = (-1) ** k0 * mp.e**lf * mp.cos(th / 2) ** (2 * lmin - 2 * k0 + M - Mp) * mp.sin(th / 2) ** (2 * k0 - M + Mp)
+        prev = mp.mpf(0)
+        tot = mp.mpc(coef[0]) * (-1) ** m * mp.sqrt((2 * lmin + 1) / (4 * mp.pi)) * cur
+        for ell in range(lmin, lmax):
+            L = mp.mpf(ell)
+            D = L * mp.sqrt(((L + 1) ** 2 - M * M) * ((L + 1) ** 2 - Mp * Mp))
+            A, C = (2 * L + 1) * L * (L + 1) / D, -(2 * L + 1) * M * Mp / D
+            B = (L + 1) * mp.sqrt((L * L - M * M) * (L * L - Mp * Mp)) / D
+            prev, cur = cur, (A * xm + C) * cur - B * prev
+            tot += mp.mpc(coef[ell + 1 - lmin]) * (-1) ** m * mp.sqrt((2 * (ell + 1) + 1) / (4 * mp.pi)) * cur
+        out.append(tot)
+    return out
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_extended_arbiter_matches_mpmath(spin):
+    from oracle import _cref
+
+    ref = _cref.load()
+    lmax = 1500
+    geo = O.Rings(1024)
+    x = geo.z[[0, 3, 700]]  # next to the pole, a polar cap ring, the belt
+    rng = np.random.default_rng(31)
+    K = O.alm_size(lmax)
+    for m in (0, 3, 700):
+        a = np.zeros((2, K), np.complex128)
+        n = lmax + 1 - m
+        b = O.alm_base(m, lmax)
+        a[:, b : b + n] = (rng.standard_normal((2, n)) + 1j * rng.standard_normal((2, n))) / (np.arange(m, lmax + 1) + 10)
+        if spin == 2:
+            a[:, b : b + max(0, 2 - m)] = 0
+            cp = -(a[0] + 1j * a[1])
+            lmin = max(m, 2)
+            coef = cp[b + lmin - m : b + n]
+            arb = ref.synth(2, lmax, x, a, m, m + 1, extended=True)[0][m]  # FpN: +2 channel
+            f64 = ref.synth(2, lmax, x, a, m, m + 1)[0][m]
+            exact = np.array([complex(_mp_column_sum(2, m, lmax, xx, coef)[0]) for xx in x])
+        else:
+            arb = ref.synth(0, lmax, x, a[:1], m, m + 1, extended=True)[0][m]
+            f64 = ref.synth(0, lmax, x, a[:1], m, m + 1)[0][m]
+            exact = np.array([complex(_mp_column_sum(0, m, lmax, xx, a[0, b : b + n])[0]) for xx in x])
+        scale = np.max(np.abs(exact))
+        # 80-bit evaluation: its rounding (mostly the running log-scale of the renormalised
+        # form) stays a thousand times below the FP64 differences it has to decide
+        e_arb, e_f64 = np.max(np.abs(arb - exact)) / scale, np.max(np.abs(f64 - exact)) / scale
+        print(f"spin {spin} m {m}: arbiter {e_arb:.2e}, FP64 oracle {e_f64:.2e}")
+        assert e_arb <= 5e-15, (m, e_arb)
+        assert e_f64 <= 1e-11

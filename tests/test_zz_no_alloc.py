@@ -54,14 +54,30 @@ def _noalloc_synthesis(alm, nside, lmax):
     return out
 
 
+# (nside, lmax) pairs, run back to back so each call overwrites the previous call's
+# scratch: the headline CPU case, a small one, the largest lmax the scratch holds at
+# nside 32 (deep underflow at high m, so the scaled start and its rescales run), the
+# smallest grid with lmax 0, and lmax far above the ring lengths (m mod N folds).
+CASES = ((64, 128), (8, 12), (32, 1023), (1, 0), (2, 40))
+
+
 def test_noalloc_matches_plan_synthesis_twice():
     rng = np.random.default_rng(2024)
-    for nside, lmax in ((64, 128), (8, 12)):
-        a = _alm(rng, lmax)
-        ref = _plan_synthesis(a, nside, lmax)
-        got = _noalloc_synthesis(a, nside, lmax)
-        err = float(torch.max(torch.abs(got - ref)) / torch.max(torch.abs(ref)))
-        assert err <= TOL, (nside, lmax, err)
+    for _ in range(2):
+        for nside, lmax in CASES:
+            a = _alm(rng, lmax)
+            ref = _plan_synthesis(a, nside, lmax)
+            got = _noalloc_synthesis(a, nside, lmax)
+            err = float(torch.max(torch.abs(got - ref)) / torch.max(torch.abs(ref)))
+            assert err <= TOL, (nside, lmax, err)
+
+
+def test_noalloc_matches_golden(golden):
+    """The reference's own synthesis at nside 64, lmax 128 (the CPU-runnable headline case)."""
+    a = torch.as_tensor(golden["s0_n64_l128/alm"], device="cuda")
+    got = _noalloc_synthesis(a, 64, 128).cpu().numpy()
+    ref = golden["s0_n64_l128/map"]
+    assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= TOL
 
 
 def test_noalloc_rejects_oversize():
