@@ -90,6 +90,13 @@ struct SeedParam {
     int pad;
 };
 
+// One work item of the tensor-core adjoint: order m, block lb of 128 degrees (l from
+// lmin + 128 lb), the ring chunks [c0, c1) it streams, and its row blk of the block-start
+// state table.
+struct TcaItem {
+    int m, lb, c0, c1, blk;
+};
+
 struct Plan {
     int nside, lmax, spin, precision, max_batch;
     int T;         // half-grid rings (north cap + equator) = 2 nside
@@ -145,6 +152,25 @@ struct Plan {
     int *d_tc_order;
     bool tc_owns_tables;
     int *d_err;           // device error flag
+    // tensor-core adjoint (precision BF16X3): recursion state at the start of every
+    // 128-degree block for every ring [blk][nrec][T], the items, and the BF16x3 ring-data
+    // tiles of one 16-map group [M][nchunk][12 KB]
+    long long tca_nblk;
+    int *d_tca_blk_off;     // [M] first block row of each order
+    double2 *d_tca_st;      // (mu_{l-1}, mu_{l-2}) before the block's first step
+    short *d_tca_sc;        // the state's scale exponent
+    TcaItem *d_tca_items;
+    int tca_nitems;
+    int tca_nchunk;         // ring chunks of the half grid (16 rings spin 2, 32 spin 0)
+    unsigned char *d_tca_B;
+    double2 *d_ag;          // (alpha, gamma) interleaved, packed like the alm (spin 2)
+    std::vector<int> h_tca_blk_off;
+    // tensor-core synthesis (precision BF16X3): prepared coefficient chunks of one map
+    // group, one per (order, 16 degrees from lmin) [chunk][bytes]
+    long long tcs_nchunks;
+    int *d_tcs_chunk_m;     // [tcs_nchunks] order of each chunk
+    int *d_tcs_cbase;       // [M] first chunk of each order
+    unsigned char *d_tcs_B;
     unsigned long long tc_wait_ns = 2000000000ull;  // time limit of the tensor-core kernels' waits
     int inject = 0;       // fault injection for tests (kInjectStall)
 
@@ -189,6 +215,12 @@ int launch_ring_adjoint(const Plan &p, const double *maps, double2 *F, double2 *
 int launch_start_states(const Plan &p, cudaStream_t s);
 int launch_start_states_r(const Plan &p, int R, int ntiles, int *lw, double2 *st, int *stsc, cudaStream_t s);
 int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaStream_t s);
+int launch_tc_adjoint(const Plan &p, const double2 *F, double2 *alm, int nb, cudaStream_t s);
+size_t tc_synth_chunk_bytes(int spin);
+int launch_tca_block_states(const Plan &p, cudaStream_t s);
+constexpr int kTcaLB = 128;       // degrees per tensor-core adjoint item (= MMA M)
+constexpr int kTcaMaps = 16;      // maps per tensor-core adjoint group
+constexpr int kTcaBStage = 12288; // bytes of one ring chunk's BF16x3 tiles (2 x 3 x 64 x 16 x 2)
 int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *offs, int nlen,
                            cudaStream_t s);
 constexpr int kRingGranule = 256;  // alignment of ring ranges: a multiple of every tile width

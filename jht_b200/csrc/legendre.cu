@@ -37,6 +37,7 @@
 #include <algorithm>
 
 #include "jhtb_internal.cuh"
+#include "seed.cuh"
 
 namespace jhtb {
 namespace {
@@ -105,34 +106,6 @@ LegParams make_params(const Plan &p) {
     q.adj_tiles = p.d_adj_tiles;
     q.counter = p.d_counter;
     return q;
-}
-
-// sign * exp(lg) as mant * 2^(800 sc) with |mant| in [2^-400, 2^400), sc <= 0.
-// The reduction lg - sc * 800 ln2 uses a two-part constant so it adds no error.
-__device__ __forceinline__ void make_seed(double lg, double sign, double &mant, int &sc) {
-    if (!(lg > -1.0e300)) {  // log(0): exact zero at a pole
-        mant = 0.0;
-        sc = 0;
-        return;
-    }
-    int k = (int)floor((lg + kLn2x400) / (kLogScaleHi + kLogScaleLo));
-    if (k > 0) k = 0;
-    const double dk = (double)k;
-    const double r = __dadd_rn(__dadd_rn(lg, -__dmul_rn(dk, kLogScaleHi)), -__dmul_rn(dk, kLogScaleLo));
-    mant = sign * exp(r);
-    sc = k;
-}
-
-// log|seed| for ring t: spin 0 (_recursion.py:315-317), spin +-2 (:181-187).
-// Unfused mul/add so the value is rounded exactly as jht's NumPy plan rounds it.
-__device__ __forceinline__ double seed_log0(const SeedParam &sp, int m, double logsin) {
-    return m == 0 ? sp.lf[0] : __dadd_rn(sp.lf[0], __dmul_rn((double)m, logsin));
-}
-__device__ __forceinline__ double seed_log2(const SeedParam &sp, int h, double lch, double lsh) {
-    double v = sp.lf[h];
-    if (sp.pc[h] > 0) v = __dadd_rn(v, __dmul_rn((double)sp.pc[h], lch));
-    if (sp.ps[h] > 0) v = __dadd_rn(v, __dmul_rn((double)sp.ps[h], lsh));
-    return v;
 }
 
 __device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {

@@ -100,6 +100,10 @@ void free_plan(Plan *p) {
             if (q) cudaFree(q);
     }
     if (p->d_tc_order) cudaFree(p->d_tc_order);
+    void *tca[] = {p->d_tca_blk_off, p->d_tca_st, p->d_tca_sc, p->d_tca_items, p->d_tca_B, p->d_ag,
+                   p->d_tcs_chunk_m, p->d_tcs_cbase, p->d_tcs_B};
+    for (void *q : tca)
+        if (q) cudaFree(q);
     for (auto &e : p->events) {
         cudaEventDestroy(e.start);
         cudaEventDestroy(e.stop);
@@ -172,9 +176,41 @@ int build_orders(Plan *p) {
             const int tile = (int)(i % p->tc_ntiles);
             if (tile * tw >= t0 && tile * tw < t1) so.push_back((int)i);
         }
-        std::stable_sort(so.begin(), so.end(), [&](int a, int b) { return lw[a] < lw[b]; });
+        // in order of m: the CTAs working at one time share the orders' coefficient chunks in L2
+        (void)lw;
         p->tc_norder = (int)so.size();
         if ((rc = refresh(&p->d_tc_order, so))) return rc;
+    }
+    // tensor-core adjoint: items (order, 128-degree block) in order of m, each streaming the
+    // ring chunks from the first 128-ring tile that is live in the block to the equator,
+    // clipped to the plan's ring range
+    if (p->precision == JHTB_PREC_BF16X3) {
+        const int CR = p->spin ? 16 : 32;
+        const int nt = p->a_ntiles, tw = 32 * (p->spin ? kRA2 : kRA0);
+        const std::vector<int> &lw = p->h_a_lw;
+        std::vector<TcaItem> items;
+        const int clo = t0 / CR, chi = std::min(p->tca_nchunk, (t1 + CR - 1) / CR);
+        for (int m = 0; m < M; ++m) {
+            const int lmin = p->spin ? std::max(m, 2) : m;
+            const int nblk = (L - lmin + 1 + kTcaLB - 1) / kTcaLB;
+            for (int lb = 0; lb < nblk; ++lb) {
+                const int l0 = lmin + lb * kTcaLB;
+                int first = nt;
+                for (int tile = 0; tile < nt; ++tile)
+                    if (lw[(long long)m * nt + tile] < l0 + kTcaLB) { first = tile; break; }
+                TcaItem it;
+                it.m = m;
+                it.lb = lb;
+                it.c0 = std::max(clo, std::min(chi, first * tw / CR));
+                it.c1 = chi;
+                it.blk = p->h_tca_blk_off[m] + lb;
+                items.push_back(it);
+            }
+        }
+        p->tca_nitems = (int)items.size();
+        if (p->d_tca_items) cudaFree(p->d_tca_items);
+        p->d_tca_items = nullptr;
+        if ((rc = upload(&p->d_tca_items, items, bytes))) return rc;
     }
     // azimuthal stage: the range's northern rings and their southern mirrors
     if (p->d_ring_list) cudaFree(p->d_ring_list);
@@ -380,6 +416,47 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
             JHTB_CUDA_TRY(cudaMemcpy(p->h_tc_lw.data(), p->d_tc_lw, sizeof(int) * nitems, cudaMemcpyDeviceToHost));
         }
     }
+    if (p->precision == JHTB_PREC_BF16X3) {
+        // tensor-core adjoint: recursion state at every 128-degree block start, every ring
+        const int nrec = spin ? 2 : 1;
+        std::vector<int> off(M);
+        long long nblk = 0;
+        for (int m = 0; m < M; ++m) {
+            off[m] = (int)nblk;
+            nblk += (L - seeds[m].lmin + 1 + kTcaLB - 1) / kTcaLB;
+        }
+        p->tca_nblk = nblk;
+        p->h_tca_blk_off = off;
+        if ((rc = upload(&p->d_tca_blk_off, off, bytes))) return rc;
+        const size_t nel = (size_t)nblk * nrec * T;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_st, sizeof(double2) * nel));
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_sc, sizeof(short) * nel));
+        bytes += (sizeof(double2) + sizeof(short)) * nel;
+        if (spin) {
+            std::vector<double2> ag(K);
+            for (long long i = 0; i < K; ++i) ag[i] = make_double2(alpha[i], gamma[i]);
+            if ((rc = upload(&p->d_ag, ag, bytes))) return rc;
+        }
+        if ((rc = launch_tca_block_states(*p, 0))) return rc;
+        JHTB_CUDA_TRY(cudaDeviceSynchronize());
+        // tensor-core synthesis: prepared coefficient chunks of 16 degrees per order
+        std::vector<int> cbase(M), chunk_m;
+        for (int m = 0; m < M; ++m) {
+            cbase[m] = (int)chunk_m.size();
+            const int nck = (L - seeds[m].lmin + 1 + 15) / 16;
+            for (int c = 0; c < nck; ++c) chunk_m.push_back(m);
+        }
+        p->tcs_nchunks = (long long)chunk_m.size();
+        if ((rc = upload(&p->d_tcs_cbase, cbase, bytes))) return rc;
+        if ((rc = upload(&p->d_tcs_chunk_m, chunk_m, bytes))) return rc;
+        const size_t cb = (size_t)p->tcs_nchunks * tc_synth_chunk_bytes(spin);
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tcs_B, cb));
+        bytes += cb;
+        p->tca_nchunk = (T + (spin ? 16 : 32) - 1) / (spin ? 16 : 32);
+        const size_t bt = (size_t)M * p->tca_nchunk * kTcaBStage;
+        JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_B, bt));
+        bytes += bt;
+    }
     p->ring_t0 = 0;
     p->ring_t1 = T;
     if ((rc = build_orders(p))) return rc;
@@ -437,7 +514,7 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
     p->chunk = std::max(1, p->max_batch);
     JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_F, f_per_map * p->chunk));
     bytes += f_per_map * p->chunk;
-    {
+    if (p->precision == JHTB_PREC_FP64) {  // partial rows of the FP64 adjoint (the tensor-core one needs none)
         const size_t part = sizeof(double2) * (size_t)p->nsuper * p->ncomp * p->K * p->chunk;
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_part, part));
         bytes += part;
@@ -621,7 +698,9 @@ int jhtb_legendre_adjoint(jhtb_plan *plan, const void *rings, void *alm, int bat
     for (int b0 = 0; b0 < batch; b0 += p.chunk) {
         const int nb = std::min(p.chunk, batch - b0);
         StageTimer t(p, s, kStageLegAdj);
-        const int rc = launch_legendre_adjoint(p, F + (size_t)b0 * f_map, a + (size_t)b0 * p.ncomp * p.K, nb, s);
+        const int rc = p.precision == JHTB_PREC_BF16X3
+                           ? launch_tc_adjoint(p, F + (size_t)b0 * f_map, a + (size_t)b0 * p.ncomp * p.K, nb, s)
+                           : launch_legendre_adjoint(p, F + (size_t)b0 * f_map, a + (size_t)b0 * p.ncomp * p.K, nb, s);
         if (rc) return rc;
     }
     return JHTB_OK;
@@ -684,7 +763,8 @@ int jhtb_adjoint_synthesis(jhtb_plan *plan, const void *maps, void *alm, int bat
         if (rc) return rc;
         {
             StageTimer t(p, s, kStageLegAdj);
-            rc = launch_legendre_adjoint(p, p.d_F, a + (size_t)b0 * p.ncomp * p.K, nb, s);
+            rc = p.precision == JHTB_PREC_BF16X3 ? launch_tc_adjoint(p, p.d_F, a + (size_t)b0 * p.ncomp * p.K, nb, s)
+                                                 : launch_legendre_adjoint(p, p.d_F, a + (size_t)b0 * p.ncomp * p.K, nb, s);
         }
         if (rc) return rc;
     }

@@ -1,0 +1,652 @@
+// Batched mixed-precision adjoint Legendre stage on the 5th-generation tensor cores.
+//
+// The adjoint contracts over rings (jht _recursion.py:472-497 spin 0, :546-572 spin 2),
+// while the recursion runs over l.  For one order m and a block of 128 degrees the
+// contraction of 16 maps is a GEMM whose reduction dimension is the rings:
+//     D[l, n] = sum_t mu_l(t) V[t, n],   l = MMA M (128), n = (map, column) = MMA N (64),
+//     t = MMA K (16 rings per instruction), streamed over all live rings of the order.
+// Spin 2 runs one GEMM per recursion: D+ = Mu+ [Vpn | s Sm], D- = Mu- [Vmn | s Sp]
+// (s = (-1)^(m + lmin), north data and the south mirror's), and the two half-grid sums
+// are p2 = D+[Vpn] + (-1)^(l-lmin) D-[Sp], m2 = D-[Vmn] + (-1)^(l-lmin) D+[Sm]; spin 0
+// runs D = Mu [Vn | Vs] over two 16-ring halves of a 32-ring chunk, b = D[Vn] + (-1)^(l-lmin) D[Vs].
+//
+// Work: one item per (order m, block of 128 degrees); items are ordered by m so that the
+// CTAs working at one time share the orders' ring data in L2.  A persistent CTA per SM
+// runs four roles that meet only at mbarriers:
+//   producer warps (one stage each, round robin): thread = (ring, recursion); start from
+//     the plan's recursion state at the block's first degree (FP64, the same arithmetic as
+//     the FP64 kernels), run the block's 128 steps, round mu to FP32, split it into three
+//     BF16 parts and store them as the A operand in MN-major layout (8 consecutive degrees
+//     per 16-byte store);
+//   a loader warp: one bulk copy per stage of the chunk's BF16x3 ring-data tiles (B
+//     operand, K-major), prepared once per launch by adj_prep_kernel from the FP64 ring
+//     spectra;
+//   one MMA warp: six split products per GEMM (hh, hm, mh, hl, lh, mm), hh into a
+//     double-buffered FP32 accumulator, the five smaller ones into a correction accumulator
+//     that runs over the whole item (relative size <= 2^-8);
+//   four epilogue warps (thread = degree = tensor-memory lane): every 256 rings they fold
+//     the hh block sums, already combined into the half-grid sums, into FP64 accumulators
+//     in shared memory (FP32 rounding acts on <= 256 rings); at the item's end they add
+//     the correction sums, scale by c_l and write the item's a_lm (E, B for spin 2).
+// The item covers every ring, so no partial sums leave the chip and the result does not
+// depend on the order of the work.  Every wait is bounded (poll count and the plan's
+// watchdog time); on timeout the kernel records an error, every role leaves its loops,
+// and tensor memory is released after the issued MMAs have drained.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "jhtb_internal.cuh"
+#include "seed.cuh"
+#include "tc_common.cuh"
+
+namespace jhtb {
+namespace {
+using namespace tc;
+
+constexpr int kLB = kTcaLB;               // degrees per item = MMA M
+constexpr int kTK = 16;                   // rings per MMA = K
+constexpr int kN = 4 * kTcaMaps;          // 64 columns per GEMM = MMA N
+constexpr int kNP = 4;                    // producer warps
+constexpr int kNSA = 5;                   // A stages
+constexpr int kNSB = 3;                   // B stages
+constexpr int kATile = kLB * kTK * 2;     // one split of one A sub-tile: 4096 bytes
+constexpr int kBTile = kN * kTK * 2;      // one split of one B sub-tile: 2048 bytes
+constexpr int kAStage = 2 * 3 * kATile;   // 24 KB
+constexpr int kBStage = 2 * 3 * kBTile;   // 12 KB
+static_assert(kBStage == kTcaBStage, "B stage size");
+constexpr int kWLoad = kNP, kWMma = kNP + 1;  // then four epilogue warps
+constexpr int kThreads = (kNP + 6) * 32;
+
+template <int SPIN>
+struct AdjCfg {
+    static constexpr int NREC = SPIN ? 2 : 1;
+    static constexpr int CR = SPIN ? 16 : 32;      // rings per stage
+    static constexpr int FOLD = 256 / CR;          // stages per FP32 accumulation block (256 rings)
+    static constexpr int NACC = SPIN ? 64 : 32;    // FP64 sums per degree: (p2, m2) or b, per map
+    static constexpr int NG = SPIN ? 2 : 1;        // accumulators (GEMMs)
+    static constexpr int COL_CORR = 2 * NG * kN;   // hh buffers first: (buf * NG + g) * kN
+    static constexpr uint32_t TCOLS = SPIN ? 512 : 256;
+};
+
+template <int SPIN>
+struct AdjSmem {
+    alignas(1024) unsigned char A[kNSA][kAStage];
+    alignas(1024) unsigned char B[kNSB][kBStage];
+    double acc[AdjCfg<SPIN>::NACC][kLB];  // [sum][degree]: a warp touches 32 consecutive words
+    alignas(8) uint64_t fullA[kNSA], emptyA[kNSA], fullB[kNSB], emptyB[kNSB];
+    uint64_t accFull[2], accEmpty[2], corrEmpty, fin;
+    uint32_t taddr;
+    int fail;
+};
+
+struct AdjParams {
+    int lmax, T, nrings;
+    long long K;
+    const double *x;
+    const SeedParam *seed;
+    const double *alpha;
+    const double2 *ag;      // (alpha, gamma) interleaved (spin 2)
+    const double *cnorm;
+    const TcaItem *items;
+    int nitems;
+    const double2 *bst;     // block-start states [blk][nrec][T]
+    const short *bsc;
+    const unsigned char *Bt;  // ring-data tiles [M][nchunk][kBStage]
+    int nchunk;
+    int *err;
+    unsigned long long wait_ns;
+    int inject;
+};
+
+// kind::f16 instruction descriptor: FP32 accumulate, BF16 A (MN-major) and B (K-major).
+constexpr uint32_t kIdescAdj = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(kN >> 3) << 17) |
+                               ((uint32_t)(kLB >> 4) << 24);
+// A sub-tile, MN-major without swizzle: 8 degrees x 8 rings core matrices of 128 bytes,
+// degree groups 128 bytes apart (SBO), the two 8-ring halves 2048 bytes apart (LBO).
+constexpr uint32_t kALbo = 2048, kASbo = 128;
+__device__ __forceinline__ uint32_t amn_off(int lgrp, int ring) {  // 16-byte row of 8 degrees
+    return (uint32_t)(lgrp * kASbo + (ring & 7) * 16 + (ring >> 3) * kALbo);
+}
+
+__device__ __forceinline__ bool adj_failed(const int *f) { return __any_sync(0xffffffffu, *(volatile const int *)f != 0); }
+__device__ __forceinline__ void adj_fail(int *f, int *err) {
+    *(volatile int *)f = 1;
+    atomicExch(err, 1);
+}
+
+__device__ __forceinline__ int item_stages(const TcaItem &q) { return q.c1 > q.c0 ? q.c1 - q.c0 : 0; }
+
+// ---------------------------------------------------------------------------------
+// producers: 128 recursion steps per (ring, recursion) -> split A operand
+// ---------------------------------------------------------------------------------
+template <int SPIN, bool SLOW>
+__device__ __forceinline__ void adj_block_steps(const AdjParams &p, long long b0, int i0, int nst, int h, double x,
+                                                double &u1, double &u2, int &sc, unsigned char *As, int j, int k) {
+    const double gsg = h ? -1.0 : 1.0;
+#pragma unroll 1
+    for (int g8 = 0; g8 < kLB / 8; ++g8) {
+        const int ib = i0 + g8 * 8;
+        uint32_t pk[3][4];
+        if (ib + 8 <= nst) {
+            double t[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                if (SPIN) {
+                    const double2 c = __ldg(&p.ag[b0 + ib + q]);
+                    t[q] = fma(c.x, x, gsg * c.y);
+                } else {
+                    t[q] = __ldg(&p.alpha[b0 + ib + q]) * x;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q += 2) {
+                double v[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    double u = fma(t[q + e], u1, -u2);
+                    double prev = u1;
+                    if (SLOW) rescale(u, prev, sc);
+                    u2 = prev;
+                    u1 = u;
+                    v[e] = (SLOW && sc != 0) ? 0.0 : u;
+                }
+                split3_pair(v[0], v[1], pk[0][q / 2], pk[1][q / 2], pk[2][q / 2]);
+            }
+        } else {
+            // the block's tail past lmax: zero rows (their outputs are not written)
+#pragma unroll
+            for (int q = 0; q < 8; q += 2) {
+                double v[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int i = ib + q + e;
+                    double val = 0.0;
+                    if (i < nst) {
+                        const double tt = SPIN ? fma(__ldg(&p.ag[b0 + i]).x, x, gsg * __ldg(&p.ag[b0 + i]).y)
+                                               : __ldg(&p.alpha[b0 + i]) * x;
+                        double u = fma(tt, u1, -u2);
+                        double prev = u1;
+                        rescale(u, prev, sc);
+                        u2 = prev;
+                        u1 = u;
+                        val = sc != 0 ? 0.0 : u;
+                    }
+                    v[e] = val;
+                }
+                split3_pair(v[0], v[1], pk[0][q / 2], pk[1][q / 2], pk[2][q / 2]);
+            }
+        }
+        const uint32_t off = amn_off(g8, k);
+#pragma unroll
+        for (int sp = 0; sp < 3; ++sp) {
+            uint4 w = make_uint4(pk[sp][0], pk[sp][1], pk[sp][2], pk[sp][3]);
+            *reinterpret_cast<uint4 *>(As + j * 3 * kATile + sp * kATile + off) = w;
+        }
+    }
+}
+
+template <int SPIN>
+__device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int lane) {
+    using C = AdjCfg<SPIN>;
+    const int j = lane >> 4, k = lane & 15;
+    const int h = SPIN ? j : 0;  // recursion (spin 2: +2 for sub-tile 0, -2 for sub-tile 1)
+    unsigned gc = 0;
+    bool ok = true;
+    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
+        if (adj_failed(&sm.fail)) break;
+        const TcaItem q = p.items[it];
+        const int nstg = item_stages(q);
+        const int lmin = __ldg(&p.seed[q.m].lmin);
+        const long long b0 = alm_index(lmin, q.m, p.lmax);
+        const int nst = p.lmax - lmin + 1;
+        const int i0 = q.lb * kLB;
+        for (int s = w; s < nstg; s += kNP) {
+            const unsigned g = gc + (unsigned)s;
+            const int sA = g % kNSA;
+            const int c = q.c0 + s;
+            const int t = SPIN ? c * C::CR + k : c * C::CR + j * 16 + k;
+            // start state of this (ring, recursion) at the block's first degree
+            double x = 0.0, u1 = 0.0, u2 = 0.0;
+            int sc = 0;
+            if (t < p.T) {
+                const size_t e = ((size_t)q.blk * C::NREC + h) * p.T + t;
+                const double2 st = p.bst[e];
+                x = __ldg(&p.x[t]);
+                u1 = st.x;
+                u2 = st.y;
+                sc = p.bsc[e];
+            }
+            if (g >= (unsigned)kNSA && !mbar_wait_warp(&sm.emptyA[sA], ((g / kNSA) - 1u) & 1u, p.wait_ns)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();  // the stage's previous MMAs are complete before it is overwritten
+            unsigned char *As = sm.A[sA];
+            if (__all_sync(0xffffffffu, sc == 0))
+                adj_block_steps<SPIN, false>(p, b0, i0, nst, h, x, u1, u2, sc, As, j, k);
+            else
+                adj_block_steps<SPIN, true>(p, b0, i0, nst, h, x, u1, u2, sc, As, j, k);
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.fullA[sA]);
+        }
+        gc += (unsigned)nstg;
+    }
+    if (!ok) adj_fail(&sm.fail, p.err);
+}
+
+// ---------------------------------------------------------------------------------
+// loader: one bulk copy of the chunk's ring-data tiles per stage
+// ---------------------------------------------------------------------------------
+template <int SPIN>
+__device__ void adj_loader(const AdjParams &p, AdjSmem<SPIN> &sm, int lane) {
+    unsigned gc = 0;
+    bool ok = true;
+    if (p.inject == kInjectStall) return;  // test hook: no ring data is ever published
+    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
+        if (adj_failed(&sm.fail)) break;
+        const TcaItem q = p.items[it];
+        const int nstg = item_stages(q);
+        for (int s = 0; s < nstg; ++s) {
+            const unsigned g = gc + (unsigned)s;
+            const int sB = g % kNSB;
+            if (g >= (unsigned)kNSB && !mbar_wait_warp(&sm.emptyB[sB], ((g / kNSB) - 1u) & 1u, p.wait_ns)) {
+                ok = false;
+                break;
+            }
+            if (lane == 0) {
+                mbar_arrive_tx(&sm.fullB[sB], kBStage);
+                bulk_g2s(sm.B[sB], p.Bt + ((size_t)q.m * p.nchunk + (q.c0 + s)) * kBStage, kBStage, &sm.fullB[sB]);
+            }
+            __syncwarp();
+        }
+        gc += (unsigned)nstg;
+    }
+    if (!ok) adj_fail(&sm.fail, p.err);
+}
+
+// ---------------------------------------------------------------------------------
+// MMA warp
+// ---------------------------------------------------------------------------------
+template <int SPIN>
+__device__ void adj_mma(const AdjParams &p, AdjSmem<SPIN> &sm, uint32_t tbase, int lane) {
+    using C = AdjCfg<SPIN>;
+    unsigned gc = 0, bk = 0, ncorr = 0;
+    bool ok = true;
+    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
+        if (adj_failed(&sm.fail)) break;
+        const TcaItem q = p.items[it];
+        const int nstg = item_stages(q);
+        for (int s = 0; s < nstg; ++s) {
+            const unsigned g = gc + (unsigned)s;
+            const int sA = g % kNSA, sB = g % kNSB;
+            const bool bstart = (s % C::FOLD) == 0;
+            const bool bend = (s % C::FOLD) == C::FOLD - 1 || s == nstg - 1;
+            const unsigned kb = bk & 1u;
+            if (!mbar_wait_warp(&sm.fullA[sA], (g / kNSA) & 1u, p.wait_ns) ||
+                !mbar_wait_warp(&sm.fullB[sB], (g / kNSB) & 1u, p.wait_ns) ||
+                (bstart && bk >= 2 && !mbar_wait_warp(&sm.accEmpty[kb], ((bk >> 1) - 1u) & 1u, p.wait_ns)) ||
+                (s == 0 && ncorr > 0 && !mbar_wait_warp(&sm.corrEmpty, (ncorr - 1u) & 1u, p.wait_ns))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            if (lane == 0) {
+#pragma unroll
+                for (int jj = 0; jj < 2; ++jj) {
+                    const int gg = SPIN ? jj : 0;  // accumulator of this sub-tile
+                    const uint32_t dh = tbase + (uint32_t)((kb * C::NG + gg) * kN);
+                    const uint32_t dc = tbase + (uint32_t)(C::COL_CORR + gg * kN);
+                    const unsigned char *Aj = sm.A[sA] + jj * 3 * kATile;
+                    const unsigned char *Bj = sm.B[sB] + jj * 3 * kBTile;
+                    const uint64_t a0 = smem_desc(Aj, kALbo, kASbo), a1 = smem_desc(Aj + kATile, kALbo, kASbo),
+                                   a2 = smem_desc(Aj + 2 * kATile, kALbo, kASbo);
+                    const uint64_t c0 = smem_desc(Bj, 128, 256), c1 = smem_desc(Bj + kBTile, 128, 256),
+                                   c2 = smem_desc(Bj + 2 * kBTile, 128, 256);
+                    // first write of each accumulator starts it at zero
+                    const uint32_t acc_h = (bstart && (SPIN || jj == 0)) ? 0u : 1u;
+                    const uint32_t acc_c = (s == 0 && (SPIN || jj == 0)) ? 0u : 1u;
+                    umma_f16_ss(dh, a0, c0, kIdescAdj, acc_h);  // hh
+                    umma_f16_ss(dc, a0, c1, kIdescAdj, acc_c);  // hm
+                    umma_f16_ss(dc, a1, c0, kIdescAdj, 1u);     // mh
+                    umma_f16_ss(dc, a0, c2, kIdescAdj, 1u);     // hl
+                    umma_f16_ss(dc, a2, c0, kIdescAdj, 1u);     // lh
+                    umma_f16_ss(dc, a1, c1, kIdescAdj, 1u);     // mm
+                }
+                umma_commit(&sm.emptyA[sA]);
+                umma_commit(&sm.emptyB[sB]);
+                if (bend) umma_commit(&sm.accFull[kb]);
+            }
+            __syncwarp();
+            if (bend) ++bk;
+        }
+        if (!ok) break;
+        if (nstg > 0) ++ncorr;
+        gc += (unsigned)nstg;
+    }
+    if (!ok) adj_fail(&sm.fail, p.err);
+    // every issued MMA has completed before tensor memory is released
+    if (lane == 0) {
+        umma_commit(&sm.fin);
+        if (!mbar_wait(&sm.fin, 0u, p.wait_ns)) adj_fail(&sm.fail, p.err);  // lane 0 alone
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------
+// epilogue: fold the block sums, write the item's a_lm
+// ---------------------------------------------------------------------------------
+// Adds this lane's (degree's) half-grid sums of 8 columns (maps b0, b0 + 1) of the FP32
+// accumulators at tensor-memory column offsets cP (spin 2: D+, spin 0: D) and cM (D-).
+template <int SPIN>
+__device__ __forceinline__ void adj_fold8(double (*acc)[kLB], int row, uint32_t tP, uint32_t tM, int col, float sgn) {
+    float vp[8];
+    tmem_ld8(tP + (uint32_t)col, vp);
+    if (SPIN) {
+        float vm[8];
+        tmem_ld8(tM + (uint32_t)col, vm);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {  // two maps of 4 columns each
+            const int b = col / 4 + e;
+            const float *P = vp + 4 * e, *Mv = vm + 4 * e;
+            // p2 = D+[Vpn] + s D-[Sp],  m2 = D-[Vmn] + s D+[Sm]
+            acc[4 * b + 0][row] += (double)P[0] + (double)(sgn * Mv[2]);
+            acc[4 * b + 1][row] += (double)P[1] + (double)(sgn * Mv[3]);
+            acc[4 * b + 2][row] += (double)Mv[0] + (double)(sgn * P[2]);
+            acc[4 * b + 3][row] += (double)Mv[1] + (double)(sgn * P[3]);
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int b = col / 4 + e;
+            const float *P = vp + 4 * e;
+            acc[2 * b + 0][row] += (double)P[0] + (double)(sgn * P[2]);
+            acc[2 * b + 1][row] += (double)P[1] + (double)(sgn * P[3]);
+        }
+    }
+}
+
+template <int SPIN>
+__device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__restrict__ alm, int nb,
+                             uint32_t tbase, int warp, int lane) {
+    using C = AdjCfg<SPIN>;
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;  // degree offset in the block = tensor-memory lane
+    const uint32_t tl = tbase + ((uint32_t)(quarter * 32) << 16);
+    double(*acc)[kLB] = sm.acc;
+    unsigned bk = 0;
+    bool ok = true;
+    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
+        if (adj_failed(&sm.fail)) break;
+        const TcaItem q = p.items[it];
+        const int nstg = item_stages(q);
+        const int nfb = (nstg + C::FOLD - 1) / C::FOLD;
+        const int lmin = __ldg(&p.seed[q.m].lmin);
+        const int l = lmin + q.lb * kLB + row;
+        const float sgn = (row & 1) ? -1.0f : 1.0f;  // (-1)^(l - lmin): blocks start at even offsets
+#pragma unroll 4
+        for (int v = 0; v < C::NACC; ++v) acc[v][row] = 0.0;
+        for (int fb = 0; fb < nfb; ++fb) {
+            const unsigned kb = bk & 1u;
+            if (!mbar_wait_warp(&sm.accFull[kb], (bk >> 1) & 1u, p.wait_ns)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t hP = tl + (uint32_t)((kb * C::NG + 0) * kN);
+            const uint32_t hM = tl + (uint32_t)((kb * C::NG + (SPIN ? 1 : 0)) * kN);
+#pragma unroll 1
+            for (int col = 0; col < kN; col += 8) adj_fold8<SPIN>(acc, row, hP, hM, col, sgn);
+            if (fb == nfb - 1) {  // the item's correction sums
+                const uint32_t cP = tl + (uint32_t)C::COL_CORR, cM = tl + (uint32_t)(C::COL_CORR + (SPIN ? kN : 0));
+#pragma unroll 1
+                for (int col = 0; col < kN; col += 8) adj_fold8<SPIN>(acc, row, cP, cM, col, sgn);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&sm.accEmpty[kb]);
+                if (fb == nfb - 1) mbar_arrive(&sm.corrEmpty);
+            }
+            ++bk;
+        }
+        if (!ok) break;
+        // outputs: a_lm of this degree for every map of the group (zero for an item without
+        // live rings); spin 2: E = (-p2 - m2) c / 2, B = i (p2 - m2) c / 2 (healpix.py:353-354)
+        if (l <= p.lmax) {
+            const long long idx = alm_index(l, q.m, p.lmax);
+            const double c = __ldg(&p.cnorm[idx]);
+            for (int b = 0; b < nb; ++b) {
+                if (SPIN) {
+                    const double pr = c * acc[4 * b + 0][row], pi = c * acc[4 * b + 1][row];
+                    const double mr = c * acc[4 * b + 2][row], mi = c * acc[4 * b + 3][row];
+                    alm[((size_t)b * 2) * p.K + idx] = make_double2(0.5 * (-pr - mr), 0.5 * (-pi - mi));
+                    alm[((size_t)b * 2 + 1) * p.K + idx] = make_double2(0.5 * (-(pi - mi)), 0.5 * (pr - mr));
+                } else {
+                    alm[(size_t)b * p.K + idx] = make_double2(c * acc[2 * b][row], c * acc[2 * b + 1][row]);
+                }
+            }
+        }
+        // degrees below lmin (spin 2, m < 2) are zero
+        if (q.lb == 0 && row < lmin - q.m) {
+            const long long idx = alm_index(q.m + row, q.m, p.lmax);
+            for (int b = 0; b < nb; ++b)
+                for (int cc = 0; cc < (SPIN ? 2 : 1); ++cc)
+                    alm[((size_t)b * (SPIN ? 2 : 1) + cc) * p.K + idx] = make_double2(0.0, 0.0);
+        }
+    }
+    if (!ok) adj_fail(&sm.fail, p.err);
+}
+
+template <int SPIN>
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_adjoint_kernel(AdjParams p, double2 *__restrict__ alm, int nb) {
+    using C = AdjCfg<SPIN>;
+    using S = AdjSmem<SPIN>;
+    extern __shared__ unsigned char smem_raw[];
+    S &sm = *reinterpret_cast<S *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == kWMma) {
+        tmem_alloc(&sm.taddr, C::TCOLS);
+        tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kNSA; ++s) {
+            mbar_init(&sm.fullA[s], 1);
+            mbar_init(&sm.emptyA[s], 1);
+        }
+        for (int s = 0; s < kNSB; ++s) {
+            mbar_init(&sm.fullB[s], 1);
+            mbar_init(&sm.emptyB[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&sm.accFull[b], 1);
+            mbar_init(&sm.accEmpty[b], 4);
+        }
+        mbar_init(&sm.corrEmpty, 4);
+        mbar_init(&sm.fin, 1);
+        sm.fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = sm.taddr;
+    if (warp < kNP) {
+        adj_producer<SPIN>(p, sm, warp, lane);
+    } else if (warp == kWLoad) {
+        adj_loader<SPIN>(p, sm, lane);
+    } else if (warp == kWMma) {
+        adj_mma<SPIN>(p, sm, tbase, lane);
+    } else {
+        adj_epilogue<SPIN>(p, sm, alm, nb, tbase, warp, lane);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == kWMma) tmem_dealloc(tbase, C::TCOLS);
+}
+
+// ---------------------------------------------------------------------------------
+// ring-data tiles: FP64 ring spectra of a 16-map group -> BF16x3 B operands per
+// (order, ring chunk), in the exact shared-memory layout the MMA reads
+// ---------------------------------------------------------------------------------
+template <int SPIN>
+__global__ void __launch_bounds__(256) adj_prep_kernel(int lmax, int T, int nrings, int M, const SeedParam *__restrict__ seed,
+                                                       const double2 *__restrict__ F, int nb, int nchunk,
+                                                       unsigned char *__restrict__ Bt) {
+    __shared__ __align__(16) unsigned char tile[kBStage];
+    const long long blk = blockIdx.x;
+    const int c = (int)(blk % nchunk), m = (int)(blk / nchunk);
+    const int k = threadIdx.x & 15, b = threadIdx.x >> 4;  // ring in the sub-tile, map
+    const size_t fmap = (size_t)(SPIN ? 2 : 1) * nrings * M;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        double col[4] = {0.0, 0.0, 0.0, 0.0};
+        const int t = SPIN ? c * 16 + k : c * 32 + j * 16 + k;
+        if (t < T && b < nb) {
+            const int rs = nrings - 1 - t;
+            const bool south = t < T - 1;
+            if (SPIN) {
+                const double ssign = ((m + seed[m].lmin) & 1) ? -1.0 : 1.0;
+                // GEMM + (j = 0): [Vpn | s Sm];  GEMM - (j = 1): [Vmn | s Sp]
+                const double2 *Fn = F + (size_t)b * fmap + (size_t)j * nrings * M;
+                const double2 *Fs = F + (size_t)b * fmap + (size_t)(1 - j) * nrings * M;
+                const double2 vn = Fn[(size_t)t * M + m];
+                const double2 vs = south ? Fs[(size_t)rs * M + m] : make_double2(0.0, 0.0);
+                col[0] = vn.x;
+                col[1] = vn.y;
+                col[2] = ssign * vs.x;
+                col[3] = ssign * vs.y;
+            } else {
+                const double2 *Fb = F + (size_t)b * fmap;
+                const double2 vn = Fb[(size_t)t * M + m];
+                const double2 vs = south ? Fb[(size_t)rs * M + m] : make_double2(0.0, 0.0);
+                col[0] = vn.x;
+                col[1] = vn.y;
+                col[2] = vs.x;
+                col[3] = vs.y;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            __nv_bfloat16 vh, vm, vl;
+            split3(col[e], vh, vm, vl);
+            const uint32_t off = kmaj_off(4 * b + e, k);
+            *reinterpret_cast<__nv_bfloat16 *>(tile + j * 3 * kBTile + 0 * kBTile + off) = vh;
+            *reinterpret_cast<__nv_bfloat16 *>(tile + j * 3 * kBTile + 1 * kBTile + off) = vm;
+            *reinterpret_cast<__nv_bfloat16 *>(tile + j * 3 * kBTile + 2 * kBTile + off) = vl;
+        }
+    }
+    __syncthreads();
+    uint4 *dst = reinterpret_cast<uint4 *>(Bt + (size_t)blk * kBStage);
+    const uint4 *src = reinterpret_cast<const uint4 *>(tile);
+    for (int i = threadIdx.x; i < kBStage / 16; i += 256) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------------
+// plan creation: the recursion state at the start of every 128-degree block, every ring
+// ---------------------------------------------------------------------------------
+template <int SPIN>
+__global__ void __launch_bounds__(128) tca_block_state_kernel(int lmax, int T, const double *__restrict__ x,
+                                                              const double *__restrict__ logsin,
+                                                              const double *__restrict__ logch,
+                                                              const double *__restrict__ logsh,
+                                                              const SeedParam *__restrict__ seed,
+                                                              const double *__restrict__ alpha,
+                                                              const double *__restrict__ gamma,
+                                                              const int *__restrict__ blk_off, double2 *__restrict__ bst,
+                                                              short *__restrict__ bsc) {
+    constexpr int NREC = SPIN ? 2 : 1;
+    const int t = blockIdx.x * 128 + threadIdx.x;
+    const int h = blockIdx.y, m = blockIdx.z;
+    if (t >= T) return;
+    const SeedParam sd = seed[m];
+    const long long b0 = alm_index(sd.lmin, m, lmax);
+    const int nst = lmax - sd.lmin + 1;
+    const double xt = x[t];
+    double mant = 0.0;
+    int sc = 0;
+    const double lg = SPIN ? seed_log2(sd, h, logch[t], logsh[t]) : seed_log0(sd, m, logsin[t]);
+    make_seed(lg, sd.sign[h], mant, sc);
+    double u1 = 0.0, u2 = -mant;
+    const double gsg = h ? -1.0 : 1.0;
+    const int nblk = (nst + kLB - 1) / kLB;
+    for (int lb = 0; lb < nblk; ++lb) {
+        const size_t e = ((size_t)(blk_off[m] + lb) * NREC + h) * T + t;
+        bst[e] = make_double2(u1, u2);
+        bsc[e] = (short)max(sc, -32768);
+        const int i1 = min(nst, (lb + 1) * kLB);
+        for (int i = lb * kLB; i < i1; ++i) {
+            const double tt = fma(alpha[b0 + i], xt, SPIN ? gsg * gamma[b0 + i] : 0.0);
+            double u = fma(tt, u1, -u2);
+            double prev = u1;
+            rescale(u, prev, sc);
+            u2 = prev;
+            u1 = u;
+        }
+    }
+}
+
+}  // namespace
+
+int launch_tca_block_states(const Plan &p, cudaStream_t s) {
+    const dim3 grid((p.T + 127) / 128, p.spin ? 2 : 1, p.M);
+    if (p.spin)
+        tca_block_state_kernel<2><<<grid, 128, 0, s>>>(p.lmax, p.T, p.d_x, p.d_logsin, p.d_logch, p.d_logsh, p.d_seed,
+                                                        p.d_alpha, p.d_gamma, p.d_tca_blk_off, p.d_tca_st, p.d_tca_sc);
+    else
+        tca_block_state_kernel<0><<<grid, 128, 0, s>>>(p.lmax, p.T, p.d_x, p.d_logsin, p.d_logch, p.d_logsh, p.d_seed,
+                                                        p.d_alpha, p.d_gamma, p.d_tca_blk_off, p.d_tca_st, p.d_tca_sc);
+    JHTB_CUDA_TRY(cudaGetLastError());
+    return JHTB_OK;
+}
+
+template <int SPIN>
+static int launch_tca_t(const Plan &p, const double2 *F, double2 *alm, int nb, cudaStream_t s) {
+    auto k = tc_adjoint_kernel<SPIN>;
+    const int smem = (int)sizeof(AdjSmem<SPIN>) + 1024;
+    int dev = 0, nsm = 148;
+    JHTB_CUDA_TRY(cudaGetDevice(&dev));
+    JHTB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    JHTB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    AdjParams q;
+    q.lmax = p.lmax;
+    q.T = p.T;
+    q.nrings = p.nrings;
+    q.K = p.K;
+    q.x = p.d_x;
+    q.seed = p.d_seed;
+    q.alpha = p.d_alpha;
+    q.ag = p.d_ag;
+    q.cnorm = p.d_cnorm;
+    q.items = p.d_tca_items;
+    q.nitems = p.tca_nitems;
+    q.bst = p.d_tca_st;
+    q.bsc = p.d_tca_sc;
+    q.Bt = p.d_tca_B;
+    q.nchunk = p.tca_nchunk;
+    q.err = p.d_err;
+    q.wait_ns = p.tc_wait_ns;
+    q.inject = p.inject;
+    const size_t fmap = (size_t)p.ncomp * p.nrings * p.M, amap = (size_t)p.ncomp * p.K;
+    for (int b0 = 0; b0 < nb; b0 += kTcaMaps) {
+        const int cnt = std::min(kTcaMaps, nb - b0);
+        const long long nblk = (long long)p.M * p.tca_nchunk;
+        adj_prep_kernel<SPIN><<<(unsigned)nblk, 256, 0, s>>>(p.lmax, p.T, p.nrings, p.M, p.d_seed, F + b0 * fmap, cnt,
+                                                              p.tca_nchunk, p.d_tca_B);
+        JHTB_CUDA_TRY(cudaGetLastError());
+        k<<<nsm, kThreads, smem, s>>>(q, alm + b0 * amap, cnt);
+        JHTB_CUDA_TRY(cudaGetLastError());
+    }
+    return JHTB_OK;
+}
+
+int launch_tc_adjoint(const Plan &p, const double2 *F, double2 *alm, int nb, cudaStream_t s) {
+    if (nb <= 0) return JHTB_OK;
+    return p.spin ? launch_tca_t<2>(p, F, alm, nb, s) : launch_tca_t<0>(p, F, alm, nb, s);
+}
+
+}  // namespace jhtb

@@ -67,3 +67,50 @@ def test_bf16x3_batch64_at_nside512():
         err = torch.amax(torch.abs(got - ref), dim=1) / torch.amax(torch.abs(ref), dim=1)
         worst = max(worst, float(err.max()))
     assert worst <= MIXED_TOL
+
+
+def _maps(rng, B, nside, spin, amp_spread=True):
+    npix = 12 * nside * nside
+    shape = (B, npix) if spin == 0 else (B, 2, npix)
+    m = rng.standard_normal(shape)
+    if amp_spread:
+        amp = 10.0 ** rng.uniform(-2, 2, size=B)
+        m = m * amp.reshape((B,) + (1,) * (m.ndim - 1))
+    return m
+
+
+# (nside, lmax, B): partial last map group (B not a multiple of 16), lmax below one 128-degree
+# block, lmax far above nside (m mod N folds, many dead polar rings), several blocks per order
+@pytest.mark.parametrize("nside,lmax,B", [(8, 12, 2), (16, 40, 9), (64, 128, 3), (128, 256, 16), (32, 300, 17)])
+@pytest.mark.parametrize("spin", [0, 2])
+def test_bf16x3_adjoint_matches_fp64(nside, lmax, B, spin):
+    """The tensor-core adjoint (split-BF16 products, FP32 sums folded into FP64 every 256
+    rings) within 1e-6 of the FP64 adjoint for every map, amplitudes spread over 1e-2..1e2."""
+    rng = np.random.default_rng(1000 + nside + lmax + B + spin)
+    v = _maps(rng, B, nside, spin)
+    ref = jhtb.adjoint_synthesis_batch(v, nside, lmax, spin).cpu().numpy()
+    out = jhtb.adjoint_synthesis_batch(v, nside, lmax, spin, precision="bf16x3").cpu().numpy()
+    assert _lib.get_plan(nside, lmax, spin, "bf16x3", B).status() == 0
+    for b in range(B):
+        err = np.max(np.abs(out[b] - ref[b])) / np.max(np.abs(ref[b]))
+        assert err <= MIXED_TOL, (b, err)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("spin", [0, 2])
+def test_bf16x3_adjoint_batch64_at_nside512(spin):
+    """64 maps at nside 512, lmax 1024 (the batched configuration), per-map amplitudes
+    log-uniform in [1e-2, 1e2]: every adjoint within 1e-6 of FP64."""
+    nside, lmax, B = 512, 1024, 64
+    rng = np.random.default_rng(640 + spin)
+    v = torch.as_tensor(_maps(rng, B, nside, spin), device="cuda")
+    out = jhtb.adjoint_synthesis_batch(v, nside, lmax, spin, precision="bf16x3")
+    assert _lib.get_plan(nside, lmax, spin, "bf16x3", B).status() == 0
+    worst = 0.0
+    for b0 in range(0, B, 16):
+        ref = jhtb.adjoint_synthesis_batch(v[b0 : b0 + 16], nside, lmax, spin)
+        got = out[b0 : b0 + 16]
+        err = torch.amax(torch.abs(got - ref).reshape(16, -1), dim=1) / torch.amax(torch.abs(ref).reshape(16, -1), dim=1)
+        worst = max(worst, float(err.max()))
+    print(f"tensor-core adjoint, nside 512, lmax 1024, spin {spin}: worst per-map error {worst:.3e}")
+    assert worst <= MIXED_TOL
