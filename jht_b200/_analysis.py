@@ -4,10 +4,11 @@ Drop-in for jht's ``_analysis`` module (src/jht/_analysis.py:49-67):
 ``A0 = S^T W`` and ``niter`` Jacobi steps ``a += A0 (m - S a)``.  The weighted
 residual ``W (m - S a)`` runs as one FP64 kernel (``jhtb_weighted_residual``).
 
-``precision`` (extension) selects the plan of the A0 applications; the residual
-synthesis ``S a`` is always FP64, so the Jacobi fixed point is the FP64 one.  The
-library's adjoint is FP64 in every precision (the tensor-core form covers the
-synthesis only), so ``precision="bf16x3"`` gives the FP64 result here.
+``precision`` (extension) selects the arithmetic of the A0 applications: with
+``"bf16x3"`` they run as the batched tensor-core adjoint (split-BF16 products, FP32
+sums folded into FP64), while the residual synthesis ``S a`` and ``W (m - S a)``
+stay FP64, so each Jacobi step corrects the previous steps' rounding and the result
+approaches the FP64 analysis.
 """
 
 from __future__ import annotations

@@ -126,7 +126,7 @@ def _cg_batch(op, b: torch.Tensor, x: torch.Tensor, tol: float, max_iter: int):
     updates and inner products are FP64 (jax.scipy.sparse.linalg.cg as used at
     masked.py:313, :371, :438).
     """
-    r = b - op(x)
+    r = b - op(x) if bool(x.any()) else b.clone()
     p = r.clone()
     gamma = (r * r).sum(dim=1)
     thresh = tol * tol * (b * b).sum(dim=1)
@@ -145,6 +145,30 @@ def _cg_batch(op, b: torch.Tensor, x: torch.Tensor, tol: float, max_iter: int):
         active = gamma > thresh
         it += 1
     return x, {"iterations": it, "rel_residual": torch.sqrt(gamma / (b * b).sum(dim=1))}
+
+
+def _refine_batch(op64, opmx, b, x, tol, max_iter, inner_tol: float = 1e-4, max_outer: int = 30):
+    """Iterative refinement: the true residual ``b - A x`` with the FP64 operator, the
+    correction from CG on the mixed-precision operator to ``inner_tol`` of that residual,
+    until ``|b - A x| <= tol |b|`` per column (FP64 residuals and inner products
+    throughout).  The mixed operator's rounding (~1e-7) only slows the outer loop; the
+    solution is the FP64 system's.  ``iterations`` counts the mixed-operator CG steps,
+    ``outer`` the FP64 residual evaluations."""
+    bn2 = (b * b).sum(dim=1)
+    total, outer = 0, 0
+    rn2 = bn2
+    while outer < max_outer:
+        r = b - op64(x)
+        outer += 1
+        rn2 = (r * r).sum(dim=1)
+        active = rn2 > (tol * tol) * bn2
+        if not bool(active.any()) or total >= max_iter:
+            break
+        r = torch.where(active[:, None], r, torch.zeros_like(r))
+        d, info = _cg_batch(opmx, r, torch.zeros_like(r), inner_tol, max_iter - total)
+        total += int(info["iterations"])
+        x = x + torch.where(active[:, None], d, torch.zeros_like(d))
+    return x, {"iterations": total, "outer": outer, "rel_residual": torch.sqrt(rn2 / bn2)}
 
 
 def _weight_pix(nside: int, npix: int, device, inv_noise=None, mask=None, use_weights: bool = True) -> torch.Tensor:
@@ -196,7 +220,10 @@ def deconvolve_batch(maps, mask, nside: int, lmax: int, spin: int = 0, *, max_it
     ``maps``: ``(B, Npix)`` (spin 0) or ``(B, 2, Npix)``; ``mask``: ``(Npix,)``.  Each
     column runs its own CG (its own step sizes and stopping test, JAX's
     ``|r|^2 <= tol^2 |b|^2``); converged columns are frozen.  Residual updates and
-    inner products are FP64.  Returns ``(B, K)`` / ``(B, 2, K)`` a_lm.
+    inner products are FP64.  With ``precision="bf16x3"`` the operator applications
+    inside CG run on the tensor cores and an outer FP64 residual refines the solution
+    (mixed-precision iterative refinement) to the same stopping test on the FP64 system.
+    Returns ``(B, K)`` / ``(B, 2, K)`` a_lm.
     """
     _check_spin(spin)
     m = _as_map(maps)
@@ -205,9 +232,14 @@ def deconvolve_batch(maps, mask, nside: int, lmax: int, spin: int = 0, *, max_it
     mb = m.reshape(m.shape[0], ncomp, npix)
     B = mb.shape[0]
     w = _weight_pix(nside, npix, mb.device, mask=mask, use_weights=use_weights)
-    b = _real_batch(_adjoint_raw(w * mb, nside, lmax, spin, precision), lmax, spin)
+    b = _real_batch(_adjoint_raw(w * mb, nside, lmax, spin, "fp64"), lmax, spin)
     x = torch.zeros_like(b) if x0 is None else _real_batch(torch.as_tensor(x0).reshape(B, ncomp, -1).to(b.device), lmax, spin)
-    x, info = _cg_batch(lambda v: _normal(v, w, nside, lmax, spin, precision) + reg * v, b, x, tol, max_iter)
+    op64 = lambda v: _normal(v, w, nside, lmax, spin, "fp64") + reg * v  # noqa: E731
+    if precision == "fp64":
+        x, info = _cg_batch(op64, b, x, tol, max_iter)
+    else:
+        opmx = lambda v: _normal(v, w, nside, lmax, spin, precision) + reg * v  # noqa: E731
+        x, info = _refine_batch(op64, opmx, b, x, tol, max_iter)
     a = _alm_batch(x, lmax, spin)
     a = a.reshape(B, alm_size(lmax)) if spin == 0 else a
     return (a, info) if return_info else a

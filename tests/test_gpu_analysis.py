@@ -317,11 +317,15 @@ def test_constrained_realization_matches_oracle_with_the_same_sources(spin):
 
 
 @pytest.mark.slow
-def test_masked_cg_16_rhs_at_nside512_converges():
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_masked_cg_16_rhs_at_nside512_converges(precision):
     """Batched masked CG at nside 512, lmax 1024: a |cos theta| < 0.34 cut plus 200 seeded
     1-degree discs, data S a + white noise (sigma 1e-2), 16 right-hand sides to relative
     residual 1e-8 with eps = 1e-6 of the largest diagonal entry of T S^T (M W) S T^-1.
-    Every column reaches the tolerance and the returned a_lm satisfies the system."""
+    Every column reaches the tolerance and the returned a_lm satisfies the FP64 system.
+    ``bf16x3``: CG on the tensor-core operator inside FP64 iterative refinement."""
+    import time
+
     from jht_b200 import masked as MK
 
     nside, lmax, spin, B = 512, 1024, 0, 16
@@ -355,11 +359,40 @@ def test_masked_cg_16_rhs_at_nside512_converges():
     diag = MK._normal(probe, w, nside, lmax, spin, "fp64")[torch.arange(16, device="cuda"), cols]
     eps = 1e-6 * float(diag.max())
     assert 0.5 < float(diag.max()) <= 1.0 + 1e-6
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     sol, info = jhtb.deconvolve_batch(maps, mask, nside, lmax, spin, tol=1e-8, reg=eps, max_iter=6000,
-                                      return_info=True)
+                                      return_info=True, precision=precision)
+    torch.cuda.synchronize()
+    print(f"masked CG {precision}: {time.perf_counter() - t0:.1f} s, {info['iterations']} iterations, "
+          f"{info.get('outer', 0)} FP64 residuals")
     assert bool(torch.all(info["rel_residual"] <= 1e-8)), (info["iterations"], info["rel_residual"])
     x = MK._real_batch(sol.reshape(B, 1, K), lmax, spin)
     b = MK._real_batch(jhtb.healpix._adjoint_raw(w * maps.reshape(B, 1, npix), nside, lmax, spin, "fp64"), lmax, spin)
     Ax = MK._normal(x, w, nside, lmax, spin, "fp64") + eps * x
     rel = torch.linalg.norm(b - Ax, dim=1) / torch.linalg.norm(b, dim=1)
     assert float(rel.max()) <= 1e-7, float(rel.max())
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("sigma", [0.0, 1e-3])
+def test_mixed_analysis_matches_fp64_at_nside1024(sigma):
+    """Spin-0 analysis(niter=3) at nside 1024, lmax 2048 of a seeded synthesis (+ white
+    noise): the tensor-core A0 applications with FP64 residuals stay within 1e-10 of the
+    FP64 analysis (relative to the largest a_lm)."""
+    nside, lmax = 1024, 2048
+    rng = np.random.default_rng(11)
+    ell = np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
+    K = jhtb.alm_size(lmax)
+    cl = 1.0 / (ell + 10.0) ** 2
+    a = np.sqrt(cl / 2) * (rng.standard_normal(K) + 1j * rng.standard_normal(K))
+    a[: lmax + 1] = np.sqrt(cl[: lmax + 1]) * rng.standard_normal(lmax + 1)
+    m = jhtb.synthesis(a, nside, lmax, 0)
+    if sigma:
+        gen = torch.Generator("cuda").manual_seed(12)
+        m = m + sigma * torch.randn(m.shape, dtype=torch.float64, device="cuda", generator=gen)
+    ref = jhtb.analysis(m, nside, lmax, 0, niter=3)
+    got = jhtb.analysis(m, nside, lmax, 0, niter=3, precision="bf16x3")
+    err = float(torch.max(torch.abs(got - ref)) / torch.max(torch.abs(ref)))
+    print(f"mixed analysis nside 1024 lmax 2048 sigma {sigma}: {err:.3e} vs FP64")
+    assert err <= 1e-10, err
