@@ -60,6 +60,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mixed-batch", type=int, default=16, help="maps per step of the mixed-precision form (0: skip)")
     ap.add_argument("--mixed-steps", type=int, default=3)
+    ap.add_argument("--no-configs", action="store_true", help="skip the analysis and 64-map batch lines")
     ap.add_argument("--offgrid-points", type=int, default=10_000_000,
                     help="points of the secondary off-grid measurement (0: skip)")
     return ap.parse_args()
@@ -261,12 +262,108 @@ def run_mixed(args, jhtb, _lib, torch, dev, pg, nside, lmax, spin, rank, world, 
         "maps_per_step_per_gpu": B,
         "ms_per_step": ms_step,
         "vs_fp64_plain": value / fp64_value,
-        "precision": "synthesis bf16x3 (tensor cores, FP32 block sums folded into FP64); adjoint and ring FFTs FP64",
+        "precision": "synthesis and adjoint Legendre stages bf16x3 (tcgen05 split-BF16 products, FP32 block sums "
+                     "folded into FP64); recursion, ring FFTs and loss FP64",
+        "roofline": _tc_roofline(stage, nside, lmax, spin, B),
         "rel_err_synthesis_vs_fp64": {"max": float(err_m.max()), "per_map": [float(e) for e in err_m]},
         "rel_err_gradient_vs_fp64": {"max": float(err_g.max()), "per_map": [float(e) for e in err_g]},
         "avg_launch_ms": {k: v / max(n, 1) for k, (v, n) in stage.items()},
         "gpu_launches": sum(n for _, n in stage.values()),
     }
+
+
+def _peaks() -> dict:
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def _tc_roofline(stage: dict, nside: int, lmax: int, spin: int, B: int) -> dict:
+    """Tensor-pipe roofline of the mixed step's Legendre kernels: split-BF16 work per launch
+    = 6 products x (16 spin 2 / 4 spin 0) contraction flops per (l, m, ring pair) and map,
+    over all K x 2 nside triples (the dead polar triples included), against the measured
+    sustained cuBLAS bf16 rate (the kernels run inside a seconds-long step)."""
+    K = (lmax + 1) * (lmax + 2) // 2
+    per = (16.0 if spin else 4.0) * 6.0
+    work = per * K * 2 * nside * B
+    pk = _peaks()
+    peak = pk.get("bf16_tflops_sustained")
+    out = {"bound": "tensor", "unit": "TFLOP/s", "peak": peak,
+           "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained" if peak else None,
+           "flops_per_launch": work}
+    for name in ("legendre_synth", "legendre_adjoint"):
+        ms, n = stage[name]
+        if n:
+            a = work / (ms / n * 1e-3) / 1e12
+            out[name] = {"achieved": a, "frac": (a / peak) if peak else None, "avg_launch_ms": ms / n}
+    return out
+
+
+def run_configs(jhtb, _lib, torch, dev) -> dict:
+    """Secondary lines at the other configurations (device-resident inputs, CUDA events):
+    spin-0 analysis(niter=3) at nside 1024 / lmax 2048, FP64 and with tensor-core A0, and
+    64 spin-0 maps S + S^T at nside 512 / lmax 1024, FP64 and bf16x3 (per-map error)."""
+    out = {}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            r = fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return r, ev[0].elapsed_time(ev[1]) / reps
+
+    # analysis
+    nside, lmax = 1024, 2048
+    rng = np.random.default_rng(11)
+    ell = np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
+    K = jhtb.alm_size(lmax)
+    cl = 1.0 / (ell + 10.0) ** 2
+    a = np.sqrt(cl / 2) * (rng.standard_normal(K) + 1j * rng.standard_normal(K))
+    a[: lmax + 1] = np.sqrt(cl[: lmax + 1]) * rng.standard_normal(lmax + 1)
+    m = jhtb.synthesis(a, nside, lmax, 0)
+    ref, t64 = timed(lambda: jhtb.analysis(m, nside, lmax, 0, niter=3))
+    mix, tmx = timed(lambda: jhtb.analysis(m, nside, lmax, 0, niter=3, precision="bf16x3"))
+    out["analysis_n1024_l2048"] = {
+        "workload": "spin-0 analysis(niter=3, ring weights), nside 1024, lmax 2048, 1 map",
+        "fp64_ms": t64, "mixed_ms": tmx, "fp64_maps_per_s": 1e3 / t64, "mixed_maps_per_s": 1e3 / tmx,
+        "mixed_rel_err_vs_fp64": float(torch.max(torch.abs(mix - ref)) / torch.max(torch.abs(ref))),
+        "fp64_tflops": 7 * 8.0 * K * 2 * nside / (t64 * 1e-3) / 1e12,
+    }
+    del m, ref, mix
+    # batched S + S^T
+    nside, lmax, B = 512, 1024, 64
+    K = jhtb.alm_size(lmax)
+    ell = np.concatenate([np.arange(mm, lmax + 1) for mm in range(lmax + 1)])
+    amp = 10.0 ** rng.uniform(-2, 2, size=B)
+    ab = (rng.standard_normal((B, K)) + 1j * rng.standard_normal((B, K))) / (ell + 10.0) * amp[:, None]
+    ab[:, : lmax + 1] = ab[:, : lmax + 1].real
+    at = torch.as_tensor(ab, device=dev)
+
+    def sst(prec):
+        mm = jhtb.synthesis_batch(at, nside, lmax, 0, precision=prec)
+        return mm, jhtb.adjoint_synthesis_batch(mm, nside, lmax, 0, precision=prec)
+
+    (m64, b64), t64 = timed(lambda: sst("fp64"))
+    (mmx, bmx), tmx = timed(lambda: sst("bf16x3"))
+    em = torch.amax(torch.abs(mmx - m64), dim=1) / torch.amax(torch.abs(m64), dim=1)
+    eb = torch.amax(torch.abs(bmx - b64), dim=1) / torch.amax(torch.abs(b64), dim=1)
+    work = 2 * 8.0 * K * 2 * nside * B  # S and S^T, spin 0: 8 flops per triple and map
+    pk = _peaks()
+    out["batch64_n512_l1024"] = {
+        "workload": "64 spin-0 maps, synthesis + adjoint, nside 512, lmax 1024, amplitudes log-uniform 1e-2..1e2",
+        "fp64_ms": t64, "mixed_ms": tmx, "fp64_maps_per_s": B * 1e3 / t64, "mixed_maps_per_s": B * 1e3 / tmx,
+        "mixed_vs_fp64": t64 / tmx,
+        "rel_err_synthesis_max": float(em.max()), "rel_err_adjoint_max": float(eb.max()),
+        "fp64_tflops": work / (t64 * 1e-3) / 1e12,
+        "mixed_tensor_tflops": 6 * 4.0 * K * 2 * nside * B * 2 / (tmx * 1e-3) / 1e12,
+        "bf16_peak_sustained": pk.get("bf16_tflops_sustained"),
+    }
+    return out
 
 
 def run_offgrid(jhtb, torch, dev, npts: int, lmax: int = 2048, spin: int = 2, reps: int = 3) -> dict:
@@ -504,6 +601,7 @@ def main():
         return
 
     offgrid = run_offgrid(jhtb, torch, dev, args.offgrid_points) if args.offgrid_points > 0 else None
+    configs = run_configs(jhtb, _lib, torch, dev) if not args.no_configs else None
 
     cpu = None
     if not args.no_cpu_baseline:
@@ -547,6 +645,7 @@ def main():
         },
         "mixed": mixed,
         "offgrid": offgrid,
+        "configs": configs,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": sum(n for _, n in stage.values()),
         "clocks": clocks,

@@ -234,6 +234,21 @@ int jhtb_plan_status(jhtb_plan *plan, int *device_error);
  * is then undefined but the context stays usable. */
 int jhtb_plan_set_watchdog(jhtb_plan *plan, int64_t timeout_ns);
 
+/* Tuning knobs (no counterpart in jht; chosen per configuration by jht_b200.autotune and
+ * kept in its table).  None changes the transform, only the speed and, for the
+ * tensor-core folds, the rounding (every allowed value keeps it within the tested bound):
+ *   JHTB_TUNE_TC_FOLD   degrees per FP32 accumulation block of the tensor-core synthesis
+ *                       (multiple of 16, default 256);
+ *   JHTB_TUNE_TCA_FOLD  rings per FP32 accumulation block of the tensor-core adjoint
+ *                       (multiple of 32, default 256);
+ *   JHTB_TUNE_TC_GROUP  maps per tensor-core synthesis group, 8 or 16 (default 16);
+ *   JHTB_TUNE_LEG_CTAS  CTAs per SM of the FP64 Legendre kernels, 0 = all that fit (default). */
+#define JHTB_TUNE_TC_FOLD 1
+#define JHTB_TUNE_TCA_FOLD 2
+#define JHTB_TUNE_TC_GROUP 3
+#define JHTB_TUNE_LEG_CTAS 4
+int jhtb_plan_set_tuning(jhtb_plan *plan, int key, int value);
+
 /* Fault injection for tests of that failure path (no GPU fault is raised).
  * JHTB_FAULT_STALL: the tensor-core kernels' operand builders publish nothing, so the
  * waits on them run out after the watchdog limit.  0 switches injection off. */

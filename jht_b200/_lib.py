@@ -24,6 +24,7 @@ JHTB_ERR_CUDA = -3
 JHTB_ERR_NOMEM = -4
 
 PRECISIONS = {"fp64": 0, "fp32": 1, "bf16x3": 2}
+TUNE_KEYS = {"tc_fold": 1, "tca_fold": 2, "tc_group": 3, "leg_ctas": 4}
 TC_MAPS = 16  # maps per tensor-core GEMM group (kTcMaps in the CUDA sources)
 
 # every exported symbol of include/jhtb.h (checked by the CPU test suite)
@@ -45,6 +46,7 @@ EXPORTS = (
     "jhtb_plan_status",
     "jhtb_plan_set_watchdog",
     "jhtb_plan_inject_fault",
+    "jhtb_plan_set_tuning",
     "jhtb_plan_ring_costs",
     "jhtb_plan_set_ring_range",
     "jhtb_plan_create_rings",
@@ -108,6 +110,7 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_plan_status": (i32, [vp, ctypes.POINTER(i32)]),
             "jhtb_plan_set_watchdog": (i32, [vp, i64]),
             "jhtb_plan_inject_fault": (i32, [vp, i32]),
+            "jhtb_plan_set_tuning": (i32, [vp, i32, i32]),
             "jhtb_plan_ring_costs": (i32, [vp, i32, ctypes.POINTER(i64), i32]),
             "jhtb_plan_set_ring_range": (i32, [vp, i32, i32]),
             "jhtb_plan_create_rings": (i32, [i32, i32, i32, i32, i32, ctypes.POINTER(HostTables),
@@ -247,6 +250,14 @@ class Plan:
         """Time limit (ns) of the tensor-core kernels' bounded waits (default 2 s)."""
         check(self.lib.jhtb_plan_set_watchdog(self.handle, int(timeout_ns)), "jhtb_plan_set_watchdog")
 
+    def set_tuning(self, **knobs: int) -> None:
+        """Apply tuning knobs (tc_fold, tca_fold, tc_group, leg_ctas); see jhtb.h."""
+        for k, v in knobs.items():
+            if k not in TUNE_KEYS:
+                raise ValueError(f"unknown tuning knob {k!r}; expected one of {tuple(TUNE_KEYS)}")
+            check(self.lib.jhtb_plan_set_tuning(self.handle, TUNE_KEYS[k], int(v)), "jhtb_plan_set_tuning")
+        self.tuning = dict(getattr(self, "tuning", {}), **knobs)
+
     def inject_fault(self, kind: int) -> None:
         """Test hook: 1 makes the tensor-core kernels' waits run out (see jhtb.h); 0 turns it off."""
         check(self.lib.jhtb_plan_inject_fault(self.handle, int(kind)), "jhtb_plan_inject_fault")
@@ -324,6 +335,11 @@ def get_plan(nside: int, lmax: int, spin: int, precision: str = "fp64", batch: i
             if plan is not None:
                 plan.close()
             plan = Plan(nside, lmax, spin, precision, max_batch=want, device=dev)
+            from .autotune import lookup  # the tuned knobs of this configuration, if any
+
+            knobs = lookup(nside, lmax, spin, batch, precision)
+            if knobs:
+                plan.set_tuning(**knobs)
             _plans[key] = plan
         return plan
 

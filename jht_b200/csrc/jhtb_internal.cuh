@@ -172,6 +172,10 @@ struct Plan {
     int *d_tcs_cbase;       // [M] first chunk of each order
     unsigned char *d_tcs_B;
     unsigned long long tc_wait_ns = 2000000000ull;  // time limit of the tensor-core kernels' waits
+    // tuning (jhtb_plan_set_tuning): FP32 accumulation block of the tensor-core synthesis
+    // (degrees) and adjoint (rings), maps per tensor-core synthesis group, CTAs per SM of
+    // the FP64 persistent kernels (0 = as many as fit)
+    int tc_fold = 256, tca_fold = 256, tc_group = 16, leg_ctas = 0;
     int inject = 0;       // fault injection for tests (kInjectStall)
 
     // ring-pair range of the plan (sharding over devices): half-grid rings

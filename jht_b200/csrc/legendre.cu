@@ -844,6 +844,13 @@ int resident_blocks(Kern k) {
     return n;
 }
 
+// Persistent grid of a Legendre kernel: every resident CTA, or the plan's tuned count.
+template <typename Kern>
+int leg_grid(const Plan &p, Kern k) {
+    const int r = resident_blocks(k);
+    return persistent_grid(p.leg_ctas > 0 ? std::min(p.leg_ctas, r) : r);
+}
+
 }  // namespace
 
 int launch_start_states(const Plan &p, cudaStream_t s) {
@@ -879,10 +886,10 @@ int launch_legendre_synth(const Plan &p, const double2 *alm, double2 *F, int nb,
     LegParams q = make_params(p);
     if (p.spin == 0) {
         auto k = synth0_kernel<kR0>;
-        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, alm, F, nb);
+        k<<<leg_grid(p, k), kWarpsPerBlock * 32, 0, s>>>(q, alm, F, nb);
     } else {
         auto k = synth2_kernel<kR2>;
-        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, alm, F, nb);
+        k<<<leg_grid(p, k), kWarpsPerBlock * 32, 0, s>>>(q, alm, F, nb);
     }
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
@@ -898,10 +905,10 @@ int launch_legendre_adjoint(const Plan &p, const double2 *F, double2 *alm, int n
     q.stsc = p.d_a_stsc;
     if (p.spin == 0) {
         auto k = adj0_kernel<kRA0>;
-        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
+        k<<<leg_grid(p, k), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
     } else {
         auto k = adj2_kernel<kRA2>;
-        k<<<persistent_grid(resident_blocks(k)), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
+        k<<<leg_grid(p, k), kWarpsPerBlock * 32, 0, s>>>(q, F, p.d_part, nb);
     }
     JHTB_CUDA_TRY(cudaGetLastError());
     const long long total = (long long)nb * p.K;

@@ -788,6 +788,33 @@ int jhtb_plan_set_watchdog(jhtb_plan *plan, int64_t timeout_ns) {
     return JHTB_OK;
 }
 
+int jhtb_plan_set_tuning(jhtb_plan *plan, int key, int value) {
+    if (!plan) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_tuning: NULL plan");
+    Plan &p = *reinterpret_cast<Plan *>(plan);
+    switch (key) {
+        case JHTB_TUNE_TC_FOLD:
+            if (value < 16 || value > 4096 || value % 16)
+                return fail(JHTB_ERR_INVALID, "jhtb_plan_set_tuning: TC_FOLD must be a multiple of 16 in [16, 4096]");
+            p.tc_fold = value;
+            return JHTB_OK;
+        case JHTB_TUNE_TCA_FOLD:
+            if (value < 32 || value > 8192 || value % 32)
+                return fail(JHTB_ERR_INVALID, "jhtb_plan_set_tuning: TCA_FOLD must be a multiple of 32 in [32, 8192]");
+            p.tca_fold = value;
+            return JHTB_OK;
+        case JHTB_TUNE_TC_GROUP:
+            if (value != 8 && value != 16) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_tuning: TC_GROUP must be 8 or 16");
+            p.tc_group = value;
+            return JHTB_OK;
+        case JHTB_TUNE_LEG_CTAS:
+            if (value < 0 || value > 16) return fail(JHTB_ERR_INVALID, "jhtb_plan_set_tuning: LEG_CTAS must be in [0, 16]");
+            p.leg_ctas = value;
+            return JHTB_OK;
+        default:
+            return fail(JHTB_ERR_INVALID, "jhtb_plan_set_tuning: unknown key " + std::to_string(key));
+    }
+}
+
 int jhtb_plan_inject_fault(jhtb_plan *plan, int kind) {
     if (!plan) return fail(JHTB_ERR_INVALID, "jhtb_plan_inject_fault: NULL plan");
     if (kind != 0 && kind != JHTB_FAULT_STALL)

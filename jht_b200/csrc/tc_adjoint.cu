@@ -63,7 +63,6 @@ template <int SPIN>
 struct AdjCfg {
     static constexpr int NREC = SPIN ? 2 : 1;
     static constexpr int CR = SPIN ? 16 : 32;      // rings per stage
-    static constexpr int FOLD = 256 / CR;          // stages per FP32 accumulation block (256 rings)
     static constexpr int NACC = SPIN ? 64 : 32;    // FP64 sums per degree: (p2, m2) or b, per map
     static constexpr int NG = SPIN ? 2 : 1;        // accumulators (GEMMs)
     static constexpr int COL_CORR = 2 * NG * kN;   // hh buffers first: (buf * NG + g) * kN
@@ -98,6 +97,7 @@ struct AdjParams {
     int *err;
     unsigned long long wait_ns;
     int inject;
+    int fold;               // stages per FP32 accumulation block
 };
 
 // kind::f16 instruction descriptor: FP32 accumulate, BF16 A (MN-major) and B (K-major).
@@ -282,8 +282,8 @@ __device__ void adj_mma(const AdjParams &p, AdjSmem<SPIN> &sm, uint32_t tbase, i
         for (int s = 0; s < nstg; ++s) {
             const unsigned g = gc + (unsigned)s;
             const int sA = g % kNSA, sB = g % kNSB;
-            const bool bstart = (s % C::FOLD) == 0;
-            const bool bend = (s % C::FOLD) == C::FOLD - 1 || s == nstg - 1;
+            const bool bstart = (s % p.fold) == 0;
+            const bool bend = (s % p.fold) == p.fold - 1 || s == nstg - 1;
             const unsigned kb = bk & 1u;
             if (!mbar_wait_warp(&sm.fullA[sA], (g / kNSA) & 1u, p.wait_ns) ||
                 !mbar_wait_warp(&sm.fullB[sB], (g / kNSB) & 1u, p.wait_ns) ||
@@ -382,7 +382,7 @@ __device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__r
         if (adj_failed(&sm.fail)) break;
         const TcaItem q = p.items[it];
         const int nstg = item_stages(q);
-        const int nfb = (nstg + C::FOLD - 1) / C::FOLD;
+        const int nfb = (nstg + p.fold - 1) / p.fold;
         const int lmin = __ldg(&p.seed[q.m].lmin);
         const int l = lmin + q.lb * kLB + row;
         const float sgn = (row & 1) ? -1.0f : 1.0f;  // (-1)^(l - lmin): blocks start at even offsets
@@ -631,6 +631,7 @@ static int launch_tca_t(const Plan &p, const double2 *F, double2 *alm, int nb, c
     q.err = p.d_err;
     q.wait_ns = p.tc_wait_ns;
     q.inject = p.inject;
+    q.fold = std::max(1, p.tca_fold / (SPIN ? 16 : 32));
     const size_t fmap = (size_t)p.ncomp * p.nrings * p.M, amap = (size_t)p.ncomp * p.K;
     for (int b0 = 0; b0 < nb; b0 += kTcaMaps) {
         const int cnt = std::min(kTcaMaps, nb - b0);

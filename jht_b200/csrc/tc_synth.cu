@@ -45,13 +45,9 @@ using namespace tc;
 
 constexpr int kTcRows = 128;     // = MMA M = rings per tile
 constexpr int kTcK = 16;         // l steps per chunk = MMA K (BF16)
-#ifndef JHTB_TC_FLUSH
-#define JHTB_TC_FLUSH 16
-#endif
 #ifndef JHTB_TC_NSA
 #define JHTB_TC_NSA 2
 #endif
-constexpr int kFlush = JHTB_TC_FLUSH;  // chunks per FP32 accumulation block (256 l)
 
 struct TcParams {
     int lmax, T, nrings, M, nside;
@@ -69,6 +65,7 @@ struct TcParams {
     int *err;
     unsigned long long wait_ns;  // time limit of every bounded wait
     int inject;                  // fault injection for tests (kInjectStall: the loader publishes nothing)
+    int flush;                   // chunks of 16 degrees per FP32 accumulation block
 };
 
 template <int SPIN, int BM>
@@ -294,11 +291,11 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
                 mbar_arrive(&sm.emptyB[sB]);
             }
             const bool last = c == q.nck - 1;
-            if ((c % kFlush) == kFlush - 1 || last) {
+            if ((c % p.flush) == p.flush - 1 || last) {
                 const unsigned kb = bk & 1u;
                 if (!mbar_wait_warp(&sm.accFull[kb], (bk >> 1) & 1u, p.wait_ns)) { ok = false; break; }
                 tc_fence_after();
-                const bool first_block = c < kFlush;
+                const bool first_block = c < p.flush;
 #pragma unroll 1
                 for (int e = 0; e < CH; ++e) {
                     const int j = j0 + e;
@@ -395,8 +392,8 @@ __device__ void tc_mma(const TcParams &p, TcSmem<SPIN, BM> &sm, uint32_t tbase, 
         const TcItem q = tc_item_of(p, __ldg(&p.order[it]));
         for (int c = 0; c < q.nck; ++c, ++gc) {
             const int sA = gc % C::NSA, sB = gc % C::NSB;
-            const bool bstart = (c % kFlush) == 0;
-            const bool bend = (c % kFlush) == kFlush - 1 || c == q.nck - 1;
+            const bool bstart = (c % p.flush) == 0;
+            const bool bend = (c % p.flush) == p.flush - 1 || c == q.nck - 1;
             const unsigned kb = bk & 1u;
             if (!mbar_wait_warp(&sm.fullA[sA], (gc / C::NSA) & 1u, p.wait_ns) ||
                 !mbar_wait_warp(&sm.fullB[sB], (gc / C::NSB) & 1u, p.wait_ns) ||
@@ -599,10 +596,11 @@ int launch_tc_synth(const Plan &p, const double2 *alm, double2 *F, int nb, cudaS
     q.err = p.d_err;
     q.wait_ns = p.tc_wait_ns;
     q.inject = p.inject;
+    q.flush = std::max(1, p.tc_fold / kTcK);
     // whole groups of kTcMaps maps share one recursion (N = 4 kTcMaps); a remainder runs
     // in groups of 8, so a short batch does not pay for the columns of a full group
     constexpr int kSmall = 8;
-    const int nbig = kTcMaps > kSmall ? (nb / kTcMaps) * kTcMaps : 0;
+    const int nbig = (kTcMaps > kSmall && p.tc_group >= kTcMaps) ? (nb / kTcMaps) * kTcMaps : 0;
     const int nsmall = nb - nbig;
     const size_t alm_map = (size_t)p.ncomp * p.K, F_map = (size_t)p.ncomp * p.nrings * p.M;
     int rc = JHTB_OK;

@@ -114,3 +114,41 @@ def test_bf16x3_adjoint_batch64_at_nside512(spin):
         worst = max(worst, float(err.max()))
     print(f"tensor-core adjoint, nside 512, lmax 1024, spin {spin}: worst per-map error {worst:.3e}")
     assert worst <= MIXED_TOL
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_tuning_knobs_keep_the_results(spin):
+    """Every knob setting the autotuner may pick keeps the transforms: mixed precision within
+    1e-6 of FP64, FP64 bit-identical to the default launch."""
+    nside, lmax, B = 32, 96, 9
+    rng = np.random.default_rng(77 + spin)
+    a = torch.as_tensor(_alms(rng, B, lmax, spin, amp_spread=True), device="cuda").reshape(B, -1, jhtb.alm_size(lmax))
+    v = torch.as_tensor(_maps(rng, B, nside, spin), device="cuda").reshape(B, a.shape[1], -1)
+
+    def pair(plan):
+        m = torch.empty(v.shape, dtype=torch.float64, device="cuda")
+        b = torch.empty(a.shape, dtype=torch.complex128, device="cuda")
+        s = _lib.stream_ptr()
+        _lib.check(plan.lib.jhtb_synthesis(plan.handle, a.data_ptr(), m.data_ptr(), B, s), "synthesis")
+        _lib.check(plan.lib.jhtb_adjoint_synthesis(plan.handle, v.data_ptr(), b.data_ptr(), B, s), "adjoint")
+        torch.cuda.synchronize()
+        return m, b
+
+    p64 = _lib.Plan(nside, lmax, spin, "fp64", max_batch=B)
+    m0, b0 = pair(p64)
+    for c in (1, 2, 3):
+        p64.set_tuning(leg_ctas=c)
+        m1, b1 = pair(p64)
+        assert torch.equal(m0, m1) and torch.equal(b0, b1)
+    p64.close()
+    pm = _lib.Plan(nside, lmax, spin, "bf16x3", max_batch=B)
+    from jht_b200 import autotune as A
+
+    for knobs in A.candidates("bf16x3", spin) + [{"tc_fold": 128, "tca_fold": 64}]:
+        pm.set_tuning(**knobs)
+        m1, b1 = pair(pm)
+        assert pm.status() == 0
+        em = torch.amax(torch.abs(m1 - m0).reshape(B, -1), 1) / torch.amax(torch.abs(m0).reshape(B, -1), 1)
+        eb = torch.amax(torch.abs(b1 - b0).reshape(B, -1), 1) / torch.amax(torch.abs(b0).reshape(B, -1), 1)
+        assert float(em.max()) <= MIXED_TOL and float(eb.max()) <= MIXED_TOL, (knobs, float(em.max()), float(eb.max()))
+    pm.close()

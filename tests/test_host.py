@@ -240,3 +240,36 @@ def test_product_ring_weights_make_m0_quadrature_exact(nside):
     assert abs(pw.sum() - 4 * np.pi) < 1e-10
     per_ring = ring_w / geo.npix_ring
     np.testing.assert_array_equal(per_ring[: 2 * nside - 1], per_ring[::-1][: 2 * nside - 1])
+
+
+def test_tuning_table_lookup(tmp_path):
+    """The autotuner's table: exact entries, the largest tuned batch not above the
+    requested one, no entry for other precisions or geometries, unknown knobs refused."""
+    import json
+
+    from jht_b200 import autotune as A
+
+    t = {A.key(2048, 4096, 2, 16, "bf16x3"): {"knobs": {"tc_fold": 512, "tc_group": 16}},
+         A.key(2048, 4096, 2, 4, "bf16x3"): {"knobs": {"tc_group": 8}},
+         A.key(512, 1024, 0, 64, "fp64"): {"knobs": {"leg_ctas": 2}}}
+    assert A.lookup(2048, 4096, 2, 16, "bf16x3", t) == {"tc_fold": 512, "tc_group": 16}
+    assert A.lookup(2048, 4096, 2, 40, "bf16x3", t) == {"tc_fold": 512, "tc_group": 16}
+    assert A.lookup(2048, 4096, 2, 8, "bf16x3", t) == {"tc_group": 8}
+    assert A.lookup(2048, 4096, 2, 2, "bf16x3", t) == {}
+    assert A.lookup(2048, 4096, 2, 16, "fp64", t) == {}
+    assert A.lookup(512, 1024, 0, 64, "fp64", t) == {"leg_ctas": 2}
+    p = tmp_path / "t.json"
+    p.write_text(json.dumps(t))
+    assert A.load_table(p) == t
+    p.write_text(json.dumps({A.key(8, 12, 0, 1, "fp64"): {"knobs": {"warp_size": 3}}}))
+    with pytest.raises(ValueError):
+        A.load_table(p)
+    # the committed table only holds known knobs, and every candidate is a valid setting
+    A.load_table()
+    for prec in ("fp64", "bf16x3"):
+        for c in A.candidates(prec, 2):
+            assert set(c) <= set(A.KNOBS)
+
+
+def test_tuning_knobs_reject_null_plan(lib):
+    assert lib.jhtb_plan_set_tuning(None, 1, 256) == _lib.JHTB_ERR_INVALID
