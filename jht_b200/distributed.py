@@ -8,8 +8,8 @@ work (ring-recursion steps per group of 256 rings, which accounts for the
 underflowed polar work the kernels skip):
 
 * synthesis: each rank evaluates its rings from the full a_lm (no exchange); the
-  map is assembled with one all-reduce of the disjoint pixel blocks (or left
-  sharded, ``gather=False``);
+  map is assembled by one all-gather of every rank's own pixel blocks (each rank
+  sends only its share of the map), or left sharded (``gather=False``);
 * adjoint: each rank contracts its rings into a partial a_lm; one all-reduce (sum)
   gives S^T v.
 
@@ -26,7 +26,8 @@ import torch
 from . import _lib
 from .healpix import RingInfo, _check_spin, alm_size
 
-__all__ = ["GRANULE", "ring_partition", "ring_ranges", "ring_pixel_blocks", "all_reduce_sum", "ShardedTransform"]
+__all__ = ["GRANULE", "ring_partition", "ring_ranges", "ring_pixel_blocks", "all_reduce_sum", "gather_pixel_blocks",
+           "ShardedTransform"]
 
 GRANULE = 256  # ring ranges are aligned to the tile widths of every kernel
 
@@ -87,6 +88,37 @@ def all_reduce_sum(t: torch.Tensor, group=None) -> torch.Tensor:
     return t
 
 
+def gather_pixel_blocks(local: torch.Tensor, nside: int, ranges, rank: int, group=None) -> torch.Tensor:
+    """Assemble the full maps (..., npix) from every rank's own rings: rank r contributes the
+    pixel blocks of its half-grid range ``ranges[r]`` (and their southern mirrors), packed
+    into one buffer; one all-gather moves the packed buffers (padded to the largest share).
+    ``local`` holds this rank's rings (other pixels are ignored).  Without an initialised
+    process group (or with one rank) it returns ``local``."""
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1):
+        return local
+    world = dist.get_world_size(group)
+    blocks = [ring_pixel_blocks(nside, t0, t1) for t0, t1 in ranges]
+    sizes = [sum(p1 - p0 for p0, p1 in b) for b in blocks]
+    nmax = max(max(sizes), 1)
+    lead = local.shape[:-1]
+    mine = [local[..., p0:p1] for p0, p1 in blocks[rank]]
+    packed = torch.zeros(lead + (nmax,), dtype=local.dtype, device=local.device)
+    if mine:
+        cat = torch.cat(mine, dim=-1)
+        packed[..., : cat.shape[-1]] = cat
+    parts = [torch.empty_like(packed) for _ in range(world)]
+    dist.all_gather(parts, packed.contiguous(), group=group)
+    out = torch.zeros_like(local)
+    for r in range(world):
+        off = 0
+        for p0, p1 in blocks[r]:
+            out[..., p0:p1] = parts[r][..., off : off + (p1 - p0)]
+            off += p1 - p0
+    return out
+
+
 class ShardedTransform:
     """S and S^T of one geometry with this rank's share of the rings.
 
@@ -109,9 +141,18 @@ class ShardedTransform:
         if ring_range is None:
             if self.world > 1:
                 costs = self.plan.ring_costs(GRANULE)
-                ring_range = ring_ranges(nside, costs, self.world)[self.rank]
+                self.ranges = ring_ranges(nside, costs, self.world)
+                ring_range = self.ranges[self.rank]
             else:
                 ring_range = (0, T)
+                self.ranges = [ring_range]
+        else:
+            # every rank's explicit range is needed to assemble the map: collect them
+            self.ranges = [tuple(ring_range)] * self.world
+            if self.world > 1:
+                got = [None] * self.world
+                dist.all_gather_object(got, tuple(ring_range), group=group)
+                self.ranges = [tuple(r) for r in got]
         self.t0, self.t1 = ring_range
         if (self.t0, self.t1) != (0, T) and self.t0 < self.t1:
             self.plan.set_ring_range(self.t0, self.t1)
@@ -124,14 +165,15 @@ class ShardedTransform:
         return t.contiguous()
 
     def synthesis(self, alm: torch.Tensor, gather: bool = True) -> torch.Tensor:
-        """Map (B, ncomp, npix) of this rank's rings (zeros elsewhere), summed over ranks if `gather`."""
+        """Map (B, ncomp, npix) of this rank's rings (zeros elsewhere), or with `gather` the whole
+        map assembled from every rank's pixel blocks."""
         a = self._batched(alm.to(torch.complex128), self.K)
         B = a.shape[0]
         out = torch.zeros((B, self.ncomp, self.npix), dtype=torch.float64, device=a.device)
         if self.t0 < self.t1 and B:
             _lib.check(self.plan.lib.jhtb_synthesis(self.plan.handle, a.data_ptr(), out.data_ptr(), B, _lib.stream_ptr()),
                        "jhtb_synthesis")
-        return all_reduce_sum(out, self.group) if gather else out
+        return gather_pixel_blocks(out, self.nside, self.ranges, self.rank, self.group) if gather else out
 
     def adjoint_synthesis(self, maps: torch.Tensor) -> torch.Tensor:
         """S^T maps (B, ncomp, K): this rank's rings contracted, summed over ranks."""

@@ -80,8 +80,10 @@ def _rank_main(rank, world, port, nside, lmax, spin, q):
         mask = np.zeros(npix)
         for p0, p1 in D.ring_pixel_blocks(nside, t0, t1):
             mask[p0:p1] = 1.0
-        mine = O.synthesis(a, nside, lmax, spin) * (mask if spin == 0 else mask[None, :])
-        full_map = D.all_reduce_sum(torch.as_tensor(mine))
+        ranges = D.ring_ranges(nside, np.ones((T + 1) // 2), world, granule=2)
+        # this rank's rings, the other pixels filled with junk the gather must ignore
+        mine = np.where(mask > 0, O.synthesis(a, nside, lmax, spin), 1e30)
+        full_map = D.gather_pixel_blocks(torch.as_tensor(mine), nside, ranges, rank)
         part = O.adjoint_synthesis(v * (mask if spin == 0 else mask[None, :]), nside, lmax, spin)
         full_adj = D.all_reduce_sum(torch.as_tensor(part))
         if rank == 0:
