@@ -208,7 +208,7 @@ def dist_setup(args):
 
 
 def run_mixed(args, jhtb, _lib, torch, dev, pg, nside, lmax, spin, rank, world, fp64_ms_per_step):
-    """Batched mixed-precision step: B maps of synthesis (tensor cores) + VJP (FP64 adjoint)."""
+    """Batched mixed-precision step: B maps of synthesis and VJP with both Legendre stages on the tensor cores."""
     B = args.mixed_batch
     alm = np.stack([make_inputs(5000 + 97 * rank + b, nside, lmax)[0] for b in range(B)])
     rng = np.random.default_rng(77 + rank)

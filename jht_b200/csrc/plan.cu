@@ -33,6 +33,9 @@ int fail(int code, const std::string &msg) {
 int cuda_fail(cudaError_t e, const char *what) {
     std::string m = std::string(what) + ": " + cudaGetErrorString(e);
     set_error(m);
+    // a failed allocation (or other non-sticky error) also sets the runtime's per-thread
+    // last error; clear it so that the caller's next CUDA call does not report it again
+    (void)cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? JHTB_ERR_NOMEM : JHTB_ERR_CUDA;
 }
 

@@ -114,19 +114,24 @@ __device__ __forceinline__ uint32_t kmaj_off(int row, int k) {
     return (uint32_t)((row >> 3) * 256 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-// x ~ h + m + l with h, m, l BF16: x is rounded to FP32, then each part keeps the top
-// 16 bits of the remaining residual (a truncation, exact in FP32), so h + m + l differs
-// from x by less than 2^-24 |x|.  Returns the three parts as FP32 bit patterns whose
-// low halves are zero (the BF16 value is the high half).
+// x ~ h + m + l with h, m, l BF16: x is rounded to FP32 (the only rounding), then each
+// part is the remaining residual rounded to 8 significant bits (to nearest, ties away
+// from zero: + 0x8000 on the bit pattern).  Each residual difference is exact in FP32
+// (the two operands are within a factor of two), and the last residual has at most 8
+// significant bits, so h + m + l == (float)x exactly, with |m| <= 2^-9 |h| and
+// |l| <= 2^-17 |h| of either sign: the products the kernels leave out (ml, lm, ll) are
+// below 2^-25 of a product and average to zero.  Returns the three parts as FP32 bit
+// patterns whose low halves are zero (the BF16 value is the high half).
+__device__ __forceinline__ uint32_t bf16_rn_bits(float v) { return (__float_as_uint(v) + 0x8000u) & 0xFFFF0000u; }
 __device__ __forceinline__ void split3_bits(double xd, uint32_t &h, uint32_t &m, uint32_t &l) {
     const float x = (float)xd;
-    h = __float_as_uint(x) & 0xFFFF0000u;
+    h = bf16_rn_bits(x);
     const float r1 = x - __uint_as_float(h);
-    m = __float_as_uint(r1) & 0xFFFF0000u;
+    m = bf16_rn_bits(r1);
     const float r2 = r1 - __uint_as_float(m);
-    l = __float_as_uint(r2) & 0xFFFF0000u;
+    l = __float_as_uint(r2) & 0xFFFF0000u;  // exact: r2 has at most 8 significant bits
 }
-// BF16 of FP32 value x by truncation (used for the B tiles, same split as split3_bits)
+// The same split as BF16 values (the coefficient and ring-data tiles)
 __device__ __forceinline__ void split3(double xd, __nv_bfloat16 &h, __nv_bfloat16 &m, __nv_bfloat16 &l) {
     uint32_t hb, mb, lb;
     split3_bits(xd, hb, mb, lb);
@@ -145,7 +150,7 @@ __device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {
 }
 
 // Two values at once, packed as BF16 pairs (x0's part in the low half) from the
-// truncation split of split3_bits; only the FP64 -> FP32 rounding uses the conversion
+// split of split3_bits; only the FP64 -> FP32 rounding uses the conversion
 // pipe, the rest is integer and FP32 arithmetic.
 __device__ __forceinline__ void split3_pair(double x0d, double x1d, uint32_t &h, uint32_t &m, uint32_t &l) {
     uint32_t h0, m0, l0, h1, m1, l1;
