@@ -435,9 +435,9 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_st, sizeof(double2) * nel));
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_sc, sizeof(short) * nel));
         bytes += (sizeof(double2) + sizeof(short)) * nel;
-        if (spin) {
+        {
             std::vector<double2> ag(K);
-            for (long long i = 0; i < K; ++i) ag[i] = make_double2(alpha[i], gamma[i]);
+            for (long long i = 0; i < K; ++i) ag[i] = make_double2(alpha[i], spin ? gamma[i] : 0.0);
             if ((rc = upload(&p->d_ag, ag, bytes))) return rc;
         }
         if ((rc = launch_tca_block_states(*p, 0))) return rc;

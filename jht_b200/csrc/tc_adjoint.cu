@@ -48,9 +48,9 @@ using namespace tc;
 constexpr int kLB = kTcaLB;               // degrees per item = MMA M
 constexpr int kTK = 16;                   // rings per MMA = K
 constexpr int kN = 4 * kTcaMaps;          // 64 columns per GEMM = MMA N
-constexpr int kNP = 4;                    // producer warps
-constexpr int kNSA = 5;                   // A stages
-constexpr int kNSB = 3;                   // B stages
+constexpr int kNP = 5;                    // producer warps
+constexpr int kNSA = 6;                   // A stages
+constexpr int kNSB = 4;                   // B stages
 constexpr int kATile = kLB * kTK * 2;     // one split of one A sub-tile: 4096 bytes
 constexpr int kBTile = kN * kTK * 2;      // one split of one B sub-tile: 2048 bytes
 constexpr int kAStage = 2 * 3 * kATile;   // 24 KB
@@ -73,9 +73,9 @@ template <int SPIN>
 struct AdjSmem {
     alignas(1024) unsigned char A[kNSA][kAStage];
     alignas(1024) unsigned char B[kNSB][kBStage];
-    double acc[AdjCfg<SPIN>::NACC][kLB];  // [sum][degree]: a warp touches 32 consecutive words
+    double2 coef[2][kLB];  // (alpha, gamma) of the item's 128 steps, double-buffered over items
     alignas(8) uint64_t fullA[kNSA], emptyA[kNSA], fullB[kNSB], emptyB[kNSB];
-    uint64_t accFull[2], accEmpty[2], corrEmpty, fin;
+    uint64_t accFull[2], accEmpty[2], corrEmpty, fin, coefFull[2], coefEmpty[2];
     uint32_t taddr;
     int fail;
 };
@@ -85,8 +85,7 @@ struct AdjParams {
     long long K;
     const double *x;
     const SeedParam *seed;
-    const double *alpha;
-    const double2 *ag;      // (alpha, gamma) interleaved (spin 2)
+    const double2 *ag;      // (alpha, gamma) interleaved, packed like the alm (gamma = 0 for spin 0)
     const double *cnorm;
     const TcaItem *items;
     int nitems;
@@ -122,8 +121,8 @@ __device__ __forceinline__ int item_stages(const TcaItem &q) { return q.c1 > q.c
 // producers: 128 recursion steps per (ring, recursion) -> split A operand
 // ---------------------------------------------------------------------------------
 template <int SPIN, bool SLOW>
-__device__ __forceinline__ void adj_block_steps(const AdjParams &p, long long b0, int i0, int nst, int h, double x,
-                                                double &u1, double &u2, int &sc, unsigned char *As, int j, int k) {
+__device__ __forceinline__ void adj_block_steps(const double2 *coef, int i0, int nst, int h, double x, double &u1,
+                                                double &u2, int &sc, unsigned char *As, int j, int k) {
     const double gsg = h ? -1.0 : 1.0;
 #pragma unroll 1
     for (int g8 = 0; g8 < kLB / 8; ++g8) {
@@ -133,12 +132,8 @@ __device__ __forceinline__ void adj_block_steps(const AdjParams &p, long long b0
             double t[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                if (SPIN) {
-                    const double2 c = __ldg(&p.ag[b0 + ib + q]);
-                    t[q] = fma(c.x, x, gsg * c.y);
-                } else {
-                    t[q] = __ldg(&p.alpha[b0 + ib + q]) * x;
-                }
+                const double2 c = coef[g8 * 8 + q];
+                t[q] = SPIN ? fma(c.x, x, gsg * c.y) : c.x * x;
             }
 #pragma unroll
             for (int q = 0; q < 8; q += 2) {
@@ -164,8 +159,8 @@ __device__ __forceinline__ void adj_block_steps(const AdjParams &p, long long b0
                     const int i = ib + q + e;
                     double val = 0.0;
                     if (i < nst) {
-                        const double tt = SPIN ? fma(__ldg(&p.ag[b0 + i]).x, x, gsg * __ldg(&p.ag[b0 + i]).y)
-                                               : __ldg(&p.alpha[b0 + i]) * x;
+                        const double2 c = coef[g8 * 8 + q + e];
+                        const double tt = SPIN ? fma(c.x, x, gsg * c.y) : c.x * x;
                         double u = fma(tt, u1, -u2);
                         double prev = u1;
                         rescale(u, prev, sc);
@@ -192,16 +187,20 @@ __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int l
     using C = AdjCfg<SPIN>;
     const int j = lane >> 4, k = lane & 15;
     const int h = SPIN ? j : 0;  // recursion (spin 2: +2 for sub-tile 0, -2 for sub-tile 1)
-    unsigned gc = 0;
+    unsigned gc = 0, n = 0;      // stages and items of this CTA so far
     bool ok = true;
-    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
+    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x, ++n) {
         if (adj_failed(&sm.fail)) break;
         const TcaItem q = p.items[it];
         const int nstg = item_stages(q);
         const int lmin = __ldg(&p.seed[q.m].lmin);
-        const long long b0 = alm_index(lmin, q.m, p.lmax);
         const int nst = p.lmax - lmin + 1;
         const int i0 = q.lb * kLB;
+        const int cb = n & 1;
+        if (!mbar_wait_warp(&sm.coefFull[cb], (n >> 1) & 1u, p.wait_ns)) {
+            ok = false;
+            break;
+        }
         for (int s = w; s < nstg; s += kNP) {
             const unsigned g = gc + (unsigned)s;
             const int sA = g % kNSA;
@@ -225,30 +224,47 @@ __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int l
             tc_fence_after();  // the stage's previous MMAs are complete before it is overwritten
             unsigned char *As = sm.A[sA];
             if (__all_sync(0xffffffffu, sc == 0))
-                adj_block_steps<SPIN, false>(p, b0, i0, nst, h, x, u1, u2, sc, As, j, k);
+                adj_block_steps<SPIN, false>(sm.coef[cb], i0, nst, h, x, u1, u2, sc, As, j, k);
             else
-                adj_block_steps<SPIN, true>(p, b0, i0, nst, h, x, u1, u2, sc, As, j, k);
+                adj_block_steps<SPIN, true>(sm.coef[cb], i0, nst, h, x, u1, u2, sc, As, j, k);
             fence_async_smem();
             __syncwarp();
             if (lane == 0) mbar_arrive(&sm.fullA[sA]);
         }
+        if (!ok) break;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.coefEmpty[cb]);  // this warp is done with the item's coefficients
         gc += (unsigned)nstg;
     }
     if (!ok) adj_fail(&sm.fail, p.err);
 }
 
 // ---------------------------------------------------------------------------------
-// loader: one bulk copy of the chunk's ring-data tiles per stage
+// loader: the item's recursion coefficients, then one bulk copy of the chunk's
+// ring-data tiles per stage
 // ---------------------------------------------------------------------------------
 template <int SPIN>
 __device__ void adj_loader(const AdjParams &p, AdjSmem<SPIN> &sm, int lane) {
-    unsigned gc = 0;
+    unsigned gc = 0, n = 0;
     bool ok = true;
-    if (p.inject == kInjectStall) return;  // test hook: no ring data is ever published
-    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
+    if (p.inject == kInjectStall) return;  // test hook: no stage is ever published
+    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x, ++n) {
         if (adj_failed(&sm.fail)) break;
         const TcaItem q = p.items[it];
         const int nstg = item_stages(q);
+        const int cb = n & 1;
+        if (n >= 2 && !mbar_wait_warp(&sm.coefEmpty[cb], ((n >> 1) - 1u) & 1u, p.wait_ns)) {
+            ok = false;
+            break;
+        }
+        if (lane == 0) {
+            const int lmin = __ldg(&p.seed[q.m].lmin);
+            const int i0 = q.lb * kLB;
+            const uint32_t bytes = (uint32_t)min(kLB, p.lmax - lmin + 1 - i0) * 16u;
+            mbar_arrive_tx(&sm.coefFull[cb], bytes);
+            bulk_g2s(sm.coef[cb], p.ag + alm_index(lmin, q.m, p.lmax) + i0, bytes, &sm.coefFull[cb]);
+        }
+        __syncwarp();
         for (int s = 0; s < nstg; ++s) {
             const unsigned g = gc + (unsigned)s;
             const int sB = g % kNSB;
@@ -338,32 +354,36 @@ __device__ void adj_mma(const AdjParams &p, AdjSmem<SPIN> &sm, uint32_t tbase, i
 // ---------------------------------------------------------------------------------
 // epilogue: fold the block sums, write the item's a_lm
 // ---------------------------------------------------------------------------------
-// Adds this lane's (degree's) half-grid sums of 8 columns (maps b0, b0 + 1) of the FP32
-// accumulators at tensor-memory column offsets cP (spin 2: D+, spin 0: D) and cM (D-).
+// Adds this lane's (degree's) half-grid sums over all 64 columns of the FP32 accumulators
+// at tensor-memory addresses tP (spin 2: D+, spin 0: D) and tM (D-) into the FP64 sums,
+// held in registers (every index is fixed at compile time).
 template <int SPIN>
-__device__ __forceinline__ void adj_fold8(double (*acc)[kLB], int row, uint32_t tP, uint32_t tM, int col, float sgn) {
-    float vp[8];
-    tmem_ld8(tP + (uint32_t)col, vp);
-    if (SPIN) {
-        float vm[8];
-        tmem_ld8(tM + (uint32_t)col, vm);
+__device__ __forceinline__ void adj_fold(double (&acc)[AdjCfg<SPIN>::NACC], uint32_t tP, uint32_t tM, float sgn) {
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {  // two maps of 4 columns each
-            const int b = col / 4 + e;
-            const float *P = vp + 4 * e, *Mv = vm + 4 * e;
-            // p2 = D+[Vpn] + s D-[Sp],  m2 = D-[Vmn] + s D+[Sm]
-            acc[4 * b + 0][row] += (double)P[0] + (double)(sgn * Mv[2]);
-            acc[4 * b + 1][row] += (double)P[1] + (double)(sgn * Mv[3]);
-            acc[4 * b + 2][row] += (double)Mv[0] + (double)(sgn * P[2]);
-            acc[4 * b + 3][row] += (double)Mv[1] + (double)(sgn * P[3]);
-        }
-    } else {
+    for (int col = 0; col < kN; col += 8) {
+        float vp[8];
+        tmem_ld8(tP + (uint32_t)col, vp);
+        if (SPIN) {
+            float vm[8];
+            tmem_ld8(tM + (uint32_t)col, vm);
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const int b = col / 4 + e;
-            const float *P = vp + 4 * e;
-            acc[2 * b + 0][row] += (double)P[0] + (double)(sgn * P[2]);
-            acc[2 * b + 1][row] += (double)P[1] + (double)(sgn * P[3]);
+            for (int e = 0; e < 2; ++e) {  // two maps of 4 columns each
+                const int b = col / 4 + e;
+                const float *P = vp + 4 * e, *Mv = vm + 4 * e;
+                // p2 = D+[Vpn] + s D-[Sp],  m2 = D-[Vmn] + s D+[Sm]
+                acc[4 * b + 0] += (double)P[0] + (double)(sgn * Mv[2]);
+                acc[4 * b + 1] += (double)P[1] + (double)(sgn * Mv[3]);
+                acc[4 * b + 2] += (double)Mv[0] + (double)(sgn * P[2]);
+                acc[4 * b + 3] += (double)Mv[1] + (double)(sgn * P[3]);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int b = col / 4 + e;
+                const float *P = vp + 4 * e;
+                acc[2 * b + 0] += (double)P[0] + (double)(sgn * P[2]);
+                acc[2 * b + 1] += (double)P[1] + (double)(sgn * P[3]);
+            }
         }
     }
 }
@@ -375,7 +395,7 @@ __device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__r
     const int quarter = warp & 3;
     const int row = quarter * 32 + lane;  // degree offset in the block = tensor-memory lane
     const uint32_t tl = tbase + ((uint32_t)(quarter * 32) << 16);
-    double(*acc)[kLB] = sm.acc;
+    double acc[C::NACC];
     unsigned bk = 0;
     bool ok = true;
     for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
@@ -386,8 +406,8 @@ __device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__r
         const int lmin = __ldg(&p.seed[q.m].lmin);
         const int l = lmin + q.lb * kLB + row;
         const float sgn = (row & 1) ? -1.0f : 1.0f;  // (-1)^(l - lmin): blocks start at even offsets
-#pragma unroll 4
-        for (int v = 0; v < C::NACC; ++v) acc[v][row] = 0.0;
+#pragma unroll
+        for (int v = 0; v < C::NACC; ++v) acc[v] = 0.0;
         for (int fb = 0; fb < nfb; ++fb) {
             const unsigned kb = bk & 1u;
             if (!mbar_wait_warp(&sm.accFull[kb], (bk >> 1) & 1u, p.wait_ns)) {
@@ -397,12 +417,10 @@ __device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__r
             tc_fence_after();
             const uint32_t hP = tl + (uint32_t)((kb * C::NG + 0) * kN);
             const uint32_t hM = tl + (uint32_t)((kb * C::NG + (SPIN ? 1 : 0)) * kN);
-#pragma unroll 1
-            for (int col = 0; col < kN; col += 8) adj_fold8<SPIN>(acc, row, hP, hM, col, sgn);
+            adj_fold<SPIN>(acc, hP, hM, sgn);
             if (fb == nfb - 1) {  // the item's correction sums
                 const uint32_t cP = tl + (uint32_t)C::COL_CORR, cM = tl + (uint32_t)(C::COL_CORR + (SPIN ? kN : 0));
-#pragma unroll 1
-                for (int col = 0; col < kN; col += 8) adj_fold8<SPIN>(acc, row, cP, cM, col, sgn);
+                adj_fold<SPIN>(acc, cP, cM, sgn);
             }
             tc_fence_before();
             __syncwarp();
@@ -418,14 +436,16 @@ __device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__r
         if (l <= p.lmax) {
             const long long idx = alm_index(l, q.m, p.lmax);
             const double c = __ldg(&p.cnorm[idx]);
-            for (int b = 0; b < nb; ++b) {
+#pragma unroll
+            for (int b = 0; b < kTcaMaps; ++b) {
+                if (b >= nb) continue;
                 if (SPIN) {
-                    const double pr = c * acc[4 * b + 0][row], pi = c * acc[4 * b + 1][row];
-                    const double mr = c * acc[4 * b + 2][row], mi = c * acc[4 * b + 3][row];
+                    const double pr = c * acc[4 * b + 0], pi = c * acc[4 * b + 1];
+                    const double mr = c * acc[4 * b + 2], mi = c * acc[4 * b + 3];
                     alm[((size_t)b * 2) * p.K + idx] = make_double2(0.5 * (-pr - mr), 0.5 * (-pi - mi));
                     alm[((size_t)b * 2 + 1) * p.K + idx] = make_double2(0.5 * (-(pi - mi)), 0.5 * (pr - mr));
                 } else {
-                    alm[(size_t)b * p.K + idx] = make_double2(c * acc[2 * b][row], c * acc[2 * b + 1][row]);
+                    alm[(size_t)b * p.K + idx] = make_double2(c * acc[2 * b], c * acc[2 * b + 1]);
                 }
             }
         }
@@ -467,6 +487,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         mbar_init(&sm.corrEmpty, 4);
         mbar_init(&sm.fin, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&sm.coefFull[b], 1);
+            mbar_init(&sm.coefEmpty[b], kNP);
+        }
         sm.fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -619,7 +643,6 @@ static int launch_tca_t(const Plan &p, const double2 *F, double2 *alm, int nb, c
     q.K = p.K;
     q.x = p.d_x;
     q.seed = p.d_seed;
-    q.alpha = p.d_alpha;
     q.ag = p.d_ag;
     q.cnorm = p.d_cnorm;
     q.items = p.d_tca_items;
