@@ -56,7 +56,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--nside", type=int, default=2048)
     ap.add_argument("--lmax", type=int, default=4096)
-    ap.add_argument("--cpu-sample-m", type=int, default=48, help="orders in the CPU-baseline sample")
+    ap.add_argument("--cpu-sample-m", type=int, default=64,
+                    help="orders in the CPU-baseline sample (the same sample for cpu_baseline and --impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mixed-batch", type=int, default=16, help="maps per step of the mixed-precision form (0: skip)")
     ap.add_argument("--mixed-steps", type=int, default=3)
@@ -409,7 +410,7 @@ def main():
         t_total = time.perf_counter()
         vals = []
         for _ in range(args.steps):
-            b = cpu_baseline(args.nside, args.lmax, max(8, args.cpu_sample_m // 3))
+            b = cpu_baseline(args.nside, args.lmax, args.cpu_sample_m)
             vals.append(b["value"])
         v = statistics.median(vals)
         line = {

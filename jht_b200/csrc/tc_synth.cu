@@ -79,7 +79,7 @@ struct TcCfg {
     static constexpr int MMA_WARP = NPW + 1;
     static constexpr int NTHREADS = (NPW + 2) * 32;
     static constexpr int NSA = JHTB_TC_NSA;         // A stages (in tensor memory)
-    static constexpr int NSB = 4;                   // B stages (with the chunk's coefficients)
+    static constexpr int NSB = 6;                   // B stages (with the chunk's coefficients): deep enough to cover the bulk copies' latency
     static constexpr int BTILE = N * kTcK * 2;
     static constexpr int BBYTES = NBT * 3 * BTILE + kTcK * 16;  // tiles, then 16 (alpha, gamma) pairs
     static constexpr int BSTRIDE = (BBYTES + 1023) / 1024 * 1024;
