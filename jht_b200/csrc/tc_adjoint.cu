@@ -201,15 +201,14 @@ __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int l
             ok = false;
             break;
         }
-        for (int s = w; s < nstg; s += kNP) {
-            const unsigned g = gc + (unsigned)s;
-            const int sA = g % kNSA;
+        // start state of this (ring, recursion) at the block's first degree for stage s, loaded
+        // one stage of this warp ahead so the memory latency overlaps the previous stage
+        auto load_state = [&](int s, double &x, double &u1, double &u2, int &sc) {
             const int c = q.c0 + s;
             const int t = SPIN ? c * C::CR + k : c * C::CR + j * 16 + k;
-            // start state of this (ring, recursion) at the block's first degree
-            double x = 0.0, u1 = 0.0, u2 = 0.0;
-            int sc = 0;
-            if (t < p.T) {
+            x = u1 = u2 = 0.0;
+            sc = 0;
+            if (s < nstg && t < p.T) {
                 const size_t e = ((size_t)q.blk * C::NREC + h) * p.T + t;
                 const double2 st = p.bst[e];
                 x = __ldg(&p.x[t]);
@@ -217,6 +216,16 @@ __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int l
                 u2 = st.y;
                 sc = p.bsc[e];
             }
+        };
+        double xn, u1n, u2n;
+        int scn;
+        load_state(w, xn, u1n, u2n, scn);
+        for (int s = w; s < nstg; s += kNP) {
+            const unsigned g = gc + (unsigned)s;
+            const int sA = g % kNSA;
+            double x = xn, u1 = u1n, u2 = u2n;
+            int sc = scn;
+            load_state(s + kNP, xn, u1n, u2n, scn);
             if (g >= (unsigned)kNSA && !mbar_wait_warp(&sm.emptyA[sA], ((g / kNSA) - 1u) & 1u, p.wait_ns)) {
                 ok = false;
                 break;
