@@ -8,7 +8,8 @@ kernels (``leg_ctas``).  For one configuration (nside, lmax, spin, batch, precis
 :func:`tune` times the pair S and S^T for every candidate setting, replayed from a
 captured CUDA graph (CUDA events around the replays), keeps only candidates whose
 result stays within ``tol`` of the FP64 transforms (mixed precision; FP64 candidates are
-bit-identical by construction), and returns the fastest.  The winners live in
+bit-identical by construction; the gate is half the tested 1e-6 bound, to keep a margin
+for inputs the tuner has not seen), and returns the fastest.  The winners live in
 ``tuning.json`` next to this module, keyed ``"nside,lmax,spin,batch,precision"``;
 :func:`jht_b200._lib.get_plan` applies the entry for its configuration (the largest
 tuned batch not above the requested one) to every plan it creates.
@@ -32,6 +33,9 @@ import numpy as np
 TABLE = Path(__file__).resolve().parent / "tuning.json"
 KNOBS = ("tc_fold", "tca_fold", "tc_group", "leg_ctas")
 MIXED_TOL = 1e-6
+# a candidate must stay within half the tested bound on the tuning inputs, so that the
+# choice keeps a margin for inputs it was not tuned on
+GATE = 0.5 * MIXED_TOL
 
 _table_cache: dict | None = None
 _table_lock = threading.Lock()
@@ -140,7 +144,7 @@ def _time(plan, a, v, m_out, b_out, reps: int) -> tuple[float, bool]:
 
 
 def tune(nside: int, lmax: int, spin: int, batch: int, precision: str, reps: int = 3,
-         tol: float = MIXED_TOL, verbose: bool = False) -> dict:
+         tol: float = GATE, verbose: bool = False) -> dict:
     """Time every candidate setting and return {"knobs", "ms", "default_ms", "err", "trials"}."""
     import torch
 
