@@ -135,25 +135,23 @@ __device__ __forceinline__ void adj_block_steps(const double2 *coef, int i0, int
                 const double2 c = coef[g8 * 8 + q];
                 t[q] = SPIN ? fma(c.x, x, gsg * c.y) : c.x * x;
             }
+            double v[8];
 #pragma unroll
-            for (int q = 0; q < 8; q += 2) {
-                double v[2];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    double u = fma(t[q + e], u1, -u2);
-                    double prev = u1;
-                    if (SLOW) rescale(u, prev, sc);
-                    u2 = prev;
-                    u1 = u;
-                    v[e] = (SLOW && sc != 0) ? 0.0 : u;
-                }
-                split3_pair(v[0], v[1], pk[0][q / 2], pk[1][q / 2], pk[2][q / 2]);
+            for (int q = 0; q < 8; ++q) {
+                double u = fma(t[q], u1, -u2);
+                double prev = u1;
+                if (SLOW) rescale(u, prev, sc);
+                u2 = prev;
+                u1 = u;
+                v[q] = (SLOW && sc != 0) ? 0.0 : u;
             }
+            split3_pack8(v, pk);
         } else {
             // the block's tail past lmax: zero rows (their outputs are not written)
+            double vt[8];
 #pragma unroll
             for (int q = 0; q < 8; q += 2) {
-                double v[2];
+                double *v = vt + q;
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     const int i = ib + q + e;
@@ -170,8 +168,8 @@ __device__ __forceinline__ void adj_block_steps(const double2 *coef, int i0, int
                     }
                     v[e] = val;
                 }
-                split3_pair(v[0], v[1], pk[0][q / 2], pk[1][q / 2], pk[2][q / 2]);
             }
+            split3_pack8(vt, pk);
         }
         const uint32_t off = amn_off(g8, k);
 #pragma unroll

@@ -149,16 +149,29 @@ __device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {
     }
 }
 
-// Two values at once, packed as BF16 pairs (x0's part in the low half) from the
-// split of split3_bits; only the FP64 -> FP32 rounding uses the conversion
-// pipe, the rest is integer and FP32 arithmetic.
-__device__ __forceinline__ void split3_pair(double x0d, double x1d, uint32_t &h, uint32_t &m, uint32_t &l) {
-    uint32_t h0, m0, l0, h1, m1, l1;
-    split3_bits(x0d, h0, m0, l0);
-    split3_bits(x1d, h1, m1, l1);
-    h = __byte_perm(h0, h1, 0x7632);
-    m = __byte_perm(m0, m1, 0x7632);
-    l = __byte_perm(l0, l1, 0x7632);
+// Eight values: the eight FP64 -> FP32 conversions are issued back to back (they run on
+// a variable-latency unit, so issuing them together overlaps their latencies), then each
+// consecutive pair is split and packed as in split3_pair: pk[part][pair].
+__device__ __forceinline__ void split3_pack8(const double (&v)[8], uint32_t (&pk)[3][4]) {
+    float f[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i] = (float)v[i];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t h[2], m[2], l[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const float x = f[2 * q + e];
+            h[e] = bf16_rn_bits(x);
+            const float r1 = x - __uint_as_float(h[e]);
+            m[e] = bf16_rn_bits(r1);
+            const float r2 = r1 - __uint_as_float(m[e]);
+            l[e] = __float_as_uint(r2) & 0xFFFF0000u;
+        }
+        pk[0][q] = __byte_perm(h[0], h[1], 0x7632);
+        pk[1][q] = __byte_perm(m[0], m[1], 0x7632);
+        pk[2][q] = __byte_perm(l[0], l[1], 0x7632);
+    }
 }
 
 

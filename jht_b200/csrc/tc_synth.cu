@@ -172,17 +172,15 @@ __device__ __forceinline__ void tc_chunk(const double2 *coef, const double (&x)[
             for (int c = 0; c < CH; ++c) t[c][k] = ((J0 + c) & 1) ? fma(a.x, x[c], -a.y) : fma(a.x, x[c], a.y);
         }
         uint32_t pk[CH][3][4];
+        double v[CH][8];
 #pragma unroll
-        for (int q = 0; q < 8; q += 2) {
-            double v0[CH], v1[CH];
-            const bool d0 = FIRST && half * 8 + q < skip, d1 = FIRST && half * 8 + q + 1 < skip;
+        for (int q = 0; q < 8; ++q) {
+            const bool dead = FIRST && half * 8 + q < skip;
 #pragma unroll
-            for (int c = 0; c < CH; ++c) v0[c] = d0 ? 0.0 : tc_step<SLOW>(t[c][q], u1[c], u2[c], sc[c]);
-#pragma unroll
-            for (int c = 0; c < CH; ++c) v1[c] = d1 ? 0.0 : tc_step<SLOW>(t[c][q + 1], u1[c], u2[c], sc[c]);
-#pragma unroll
-            for (int c = 0; c < CH; ++c) split3_pair(v0[c], v1[c], pk[c][0][q / 2], pk[c][1][q / 2], pk[c][2][q / 2]);
+            for (int c = 0; c < CH; ++c) v[c][q] = dead ? 0.0 : tc_step<SLOW>(t[c][q], u1[c], u2[c], sc[c]);
         }
+#pragma unroll
+        for (int c = 0; c < CH; ++c) split3_pack8(v[c], pk[c]);
 #pragma unroll
         for (int c = 0; c < CH; ++c)
 #pragma unroll
