@@ -119,56 +119,49 @@ def _alm_batch(x: torch.Tensor, lmax: int, spin: int) -> torch.Tensor:
     return out
 
 
-def _cg_batch(op, b: torch.Tensor, x: torch.Tensor, tol: float, max_iter: int):
+def _cg_batch(op, b: torch.Tensor, x: torch.Tensor, tol: float, max_iter: int, op_true=None,
+              replace_every: int = 50):
     """Column-wise CG on (B, n) right-hand sides with JAX's stopping rule |r|^2 <= tol^2 |b|^2.
 
     Each column runs its own step sizes; converged columns are frozen.  Residual
     updates and inner products are FP64 (jax.scipy.sparse.linalg.cg as used at
-    masked.py:313, :371, :438).
+    masked.py:313, :371, :438).  With ``op_true`` (the FP64 operator, when ``op`` is a
+    mixed-precision one) the recursive residual is replaced by the true residual
+    ``b - op_true(x)`` every ``replace_every`` steps and whenever the recursive one meets the
+    test, so the stopping rule holds for the FP64 system (CG with residual replacement).
     """
-    r = b - op(x) if bool(x.any()) else b.clone()
+    def true_residual(x):
+        return b - op_true(x)
+
+    if op_true is not None:
+        r = true_residual(x) if bool(x.any()) else b.clone()
+    else:
+        r = b - op(x) if bool(x.any()) else b.clone()
     p = r.clone()
     gamma = (r * r).sum(dim=1)
     thresh = tol * tol * (b * b).sum(dim=1)
     active = gamma > thresh
-    it = 0
+    it, replaced = 0, 0
     while bool(active.any()) and it < max_iter:
         Ap = op(p)
         denom = (p * Ap).sum(dim=1)
         alpha = torch.where(active, gamma / torch.where(active, denom, torch.ones_like(denom)), torch.zeros_like(gamma))
         x = x + alpha[:, None] * p
         r = r - alpha[:, None] * Ap
+        it += 1
         g2 = (r * r).sum(dim=1)
+        if op_true is not None and (it % replace_every == 0 or not bool((active & (g2 > thresh)).any())):
+            r = torch.where(active[:, None], true_residual(x), r)
+            g2 = (r * r).sum(dim=1)
+            replaced += 1
         beta = torch.where(active, g2 / torch.where(active, gamma, torch.ones_like(gamma)), torch.zeros_like(g2))
         p = torch.where(active[:, None], r + beta[:, None] * p, p)
         gamma = torch.where(active, g2, gamma)
         active = gamma > thresh
-        it += 1
-    return x, {"iterations": it, "rel_residual": torch.sqrt(gamma / (b * b).sum(dim=1))}
-
-
-def _refine_batch(op64, opmx, b, x, tol, max_iter, inner_tol: float = 1e-4, max_outer: int = 30):
-    """Iterative refinement: the true residual ``b - A x`` with the FP64 operator, the
-    correction from CG on the mixed-precision operator to ``inner_tol`` of that residual,
-    until ``|b - A x| <= tol |b|`` per column (FP64 residuals and inner products
-    throughout).  The mixed operator's rounding (~1e-7) only slows the outer loop; the
-    solution is the FP64 system's.  ``iterations`` counts the mixed-operator CG steps,
-    ``outer`` the FP64 residual evaluations."""
-    bn2 = (b * b).sum(dim=1)
-    total, outer = 0, 0
-    rn2 = bn2
-    while outer < max_outer:
-        r = b - op64(x)
-        outer += 1
-        rn2 = (r * r).sum(dim=1)
-        active = rn2 > (tol * tol) * bn2
-        if not bool(active.any()) or total >= max_iter:
-            break
-        r = torch.where(active[:, None], r, torch.zeros_like(r))
-        d, info = _cg_batch(opmx, r, torch.zeros_like(r), inner_tol, max_iter - total)
-        total += int(info["iterations"])
-        x = x + torch.where(active[:, None], d, torch.zeros_like(d))
-    return x, {"iterations": total, "outer": outer, "rel_residual": torch.sqrt(rn2 / bn2)}
+    info = {"iterations": it, "rel_residual": torch.sqrt(gamma / (b * b).sum(dim=1))}
+    if op_true is not None:
+        info["outer"] = replaced
+    return x, info
 
 
 def _weight_pix(nside: int, npix: int, device, inv_noise=None, mask=None, use_weights: bool = True) -> torch.Tensor:
@@ -221,8 +214,9 @@ def deconvolve_batch(maps, mask, nside: int, lmax: int, spin: int = 0, *, max_it
     column runs its own CG (its own step sizes and stopping test, JAX's
     ``|r|^2 <= tol^2 |b|^2``); converged columns are frozen.  Residual updates and
     inner products are FP64.  With ``precision="bf16x3"`` the operator applications
-    inside CG run on the tensor cores and an outer FP64 residual refines the solution
-    (mixed-precision iterative refinement) to the same stopping test on the FP64 system.
+    inside CG run on the tensor cores and the recursive residual is replaced by the true
+    FP64 residual every 50 steps and before the stopping test is accepted, so the test
+    holds on the FP64 system (CG with residual replacement).
     Returns ``(B, K)`` / ``(B, 2, K)`` a_lm.
     """
     _check_spin(spin)
@@ -239,7 +233,7 @@ def deconvolve_batch(maps, mask, nside: int, lmax: int, spin: int = 0, *, max_it
         x, info = _cg_batch(op64, b, x, tol, max_iter)
     else:
         opmx = lambda v: _normal(v, w, nside, lmax, spin, precision) + reg * v  # noqa: E731
-        x, info = _refine_batch(op64, opmx, b, x, tol, max_iter)
+        x, info = _cg_batch(opmx, b, x, tol, max_iter, op_true=op64)
     a = _alm_batch(x, lmax, spin)
     a = a.reshape(B, alm_size(lmax)) if spin == 0 else a
     return (a, info) if return_info else a

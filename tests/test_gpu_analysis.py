@@ -323,7 +323,7 @@ def test_masked_cg_16_rhs_at_nside512_converges(precision):
     1-degree discs, data S a + white noise (sigma 1e-2), 16 right-hand sides to relative
     residual 1e-8 with eps = 1e-6 of the largest diagonal entry of T S^T (M W) S T^-1.
     Every column reaches the tolerance and the returned a_lm satisfies the FP64 system.
-    ``bf16x3``: CG on the tensor-core operator inside FP64 iterative refinement."""
+    ``bf16x3``: CG on the tensor-core operator with the FP64 residual replacing the recursive one."""
     import time
 
     from jht_b200 import masked as MK
