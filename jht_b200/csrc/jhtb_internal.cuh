@@ -91,10 +91,11 @@ struct SeedParam {
 };
 
 // One work item of the tensor-core adjoint: order m, block lb of 128 degrees (l from
-// lmin + 128 lb), the ring chunks [c0, c1) it streams, and its row blk of the block-start
-// state table.
+// lmin + 128 lb), the ring chunks [c0, c1) it streams, the block's first live ring chunk
+// cl (<= c0) and the offset soff of its rows in the segment-state table.
 struct TcaItem {
-    int m, lb, c0, c1, blk;
+    int m, lb, c0, c1, cl, pad;
+    long long soff;
 };
 
 struct Plan {
@@ -153,18 +154,24 @@ struct Plan {
     bool tc_owns_tables;
     int *d_err;           // device error flag
     // tensor-core adjoint (precision BF16X3): recursion state at the start of every
-    // 128-degree block for every ring [blk][nrec][T], the items, and the BF16x3 ring-data
-    // tiles of one 16-map group [M][nchunk][12 KB]
+    // 32-degree segment of every 128-degree block, for the block's live ring chunks only
+    // (rows [block][chunk - cl][segment][32 lanes], lane = recursion x 16 rings for spin 2,
+    // 32 rings for spin 0), the items, and the BF16x3 ring-data tiles of one 16-map group
+    // [M][nchunk][12 KB]
     long long tca_nblk;
-    int *d_tca_blk_off;     // [M] first block row of each order
-    double2 *d_tca_st;      // (mu_{l-1}, mu_{l-2}) before the block's first step
+    long long tca_nstate;   // rows of the segment-state table
+    int *d_tca_blk_off;     // [M] first block of each order
+    int *d_tca_blk_cl;      // [block] first live ring chunk
+    long long *d_tca_blk_soff;  // [block] first row in the segment-state table
+    double2 *d_tca_st;      // (mu_{l-1}, mu_{l-2}) before the segment's first step
     short *d_tca_sc;        // the state's scale exponent
     TcaItem *d_tca_items;
     int tca_nitems;
     int tca_nchunk;         // ring chunks of the half grid (16 rings spin 2, 32 spin 0)
     unsigned char *d_tca_B;
     double2 *d_ag;          // (alpha, gamma) interleaved, packed like the alm (spin 2)
-    std::vector<int> h_tca_blk_off;
+    std::vector<int> h_tca_blk_off, h_tca_blk_cl;
+    std::vector<long long> h_tca_blk_soff;
     // tensor-core synthesis (precision BF16X3): prepared coefficient chunks of one map
     // group, one per (order, 16 degrees from lmin) [chunk][bytes]
     long long tcs_nchunks;
@@ -223,6 +230,7 @@ int launch_tc_adjoint(const Plan &p, const double2 *F, double2 *alm, int nb, cud
 size_t tc_synth_chunk_bytes(int spin);
 int launch_tca_block_states(const Plan &p, cudaStream_t s);
 constexpr int kTcaLB = 128;       // degrees per tensor-core adjoint item (= MMA M)
+constexpr int kTcaSeg = 4;        // recursion segments per item (independent chains per thread)
 constexpr int kTcaMaps = 16;      // maps per tensor-core adjoint group
 constexpr int kTcaBStage = 12288; // bytes of one ring chunk's BF16x3 tiles (2 x 3 x 64 x 16 x 2)
 int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *offs, int nlen,

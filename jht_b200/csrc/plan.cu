@@ -103,8 +103,8 @@ void free_plan(Plan *p) {
             if (q) cudaFree(q);
     }
     if (p->d_tc_order) cudaFree(p->d_tc_order);
-    void *tca[] = {p->d_tca_blk_off, p->d_tca_st, p->d_tca_sc, p->d_tca_items, p->d_tca_B, p->d_ag,
-                   p->d_tcs_chunk_m, p->d_tcs_cbase, p->d_tcs_B};
+    void *tca[] = {p->d_tca_blk_off, p->d_tca_blk_cl, p->d_tca_blk_soff, p->d_tca_st, p->d_tca_sc, p->d_tca_items,
+                   p->d_tca_B, p->d_ag, p->d_tcs_chunk_m, p->d_tcs_cbase, p->d_tcs_B};
     for (void *q : tca)
         if (q) cudaFree(q);
     for (auto &e : p->events) {
@@ -193,20 +193,22 @@ int build_orders(Plan *p) {
         const std::vector<int> &lw = p->h_a_lw;
         std::vector<TcaItem> items;
         const int clo = t0 / CR, chi = std::min(p->tca_nchunk, (t1 + CR - 1) / CR);
+        (void)nt;
+        (void)tw;
+        (void)lw;
         for (int m = 0; m < M; ++m) {
             const int lmin = p->spin ? std::max(m, 2) : m;
             const int nblk = (L - lmin + 1 + kTcaLB - 1) / kTcaLB;
             for (int lb = 0; lb < nblk; ++lb) {
-                const int l0 = lmin + lb * kTcaLB;
-                int first = nt;
-                for (int tile = 0; tile < nt; ++tile)
-                    if (lw[(long long)m * nt + tile] < l0 + kTcaLB) { first = tile; break; }
+                const int blk = p->h_tca_blk_off[m] + lb;
                 TcaItem it;
                 it.m = m;
                 it.lb = lb;
-                it.c0 = std::max(clo, std::min(chi, first * tw / CR));
+                it.cl = p->h_tca_blk_cl[blk];
+                it.c0 = std::max(clo, std::min(chi, it.cl));
                 it.c1 = chi;
-                it.blk = p->h_tca_blk_off[m] + lb;
+                it.pad = 0;
+                it.soff = p->h_tca_blk_soff[blk];
                 items.push_back(it);
             }
         }
@@ -420,8 +422,8 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         }
     }
     if (p->precision == JHTB_PREC_BF16X3) {
-        // tensor-core adjoint: recursion state at every 128-degree block start, every ring
-        const int nrec = spin ? 2 : 1;
+        // tensor-core adjoint: recursion state at every 32-degree segment start of every
+        // 128-degree block, for the block's live ring chunks
         std::vector<int> off(M);
         long long nblk = 0;
         for (int m = 0; m < M; ++m) {
@@ -431,7 +433,39 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         p->tca_nblk = nblk;
         p->h_tca_blk_off = off;
         if ((rc = upload(&p->d_tca_blk_off, off, bytes))) return rc;
-        const size_t nel = (size_t)nblk * nrec * T;
+        // the block's first live ring chunk: the first chunk of the first ring tile of the
+        // FP64 adjoint whose first live degree lies below the block's end (tiles nearer the
+        // equator start no later); segment states are kept from that chunk to the equator
+        p->tca_nchunk = (T + (spin ? 16 : 32) - 1) / (spin ? 16 : 32);
+        {
+            const int CR = spin ? 16 : 32, nt = p->a_ntiles, tw = 32 * (spin ? kRA2 : kRA0);
+            std::vector<int> cl(nblk);
+            std::vector<long long> soff(nblk);
+            long long rows = 0;
+            for (int m = 0; m < M; ++m) {
+                const int lmin = seeds[m].lmin;
+                const int nb = (L - lmin + 1 + kTcaLB - 1) / kTcaLB;
+                for (int lb = 0; lb < nb; ++lb) {
+                    const int l0 = lmin + lb * kTcaLB;
+                    int first = nt;
+                    for (int tile = 0; tile < nt; ++tile)
+                        if (p->h_a_lw[(long long)m * nt + tile] < l0 + kTcaLB) {
+                            first = tile;
+                            break;
+                        }
+                    const long long b = off[m] + lb;
+                    cl[b] = std::min(p->tca_nchunk, (int)((long long)first * tw / CR));
+                    soff[b] = rows;
+                    rows += (long long)(p->tca_nchunk - cl[b]) * kTcaSeg * 32;
+                }
+            }
+            p->tca_nstate = rows;
+            p->h_tca_blk_cl = cl;
+            p->h_tca_blk_soff = soff;
+            if ((rc = upload(&p->d_tca_blk_cl, cl, bytes))) return rc;
+            if ((rc = upload(&p->d_tca_blk_soff, soff, bytes))) return rc;
+        }
+        const size_t nel = (size_t)std::max(1LL, p->tca_nstate);
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_st, sizeof(double2) * nel));
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_sc, sizeof(short) * nel));
         bytes += (sizeof(double2) + sizeof(short)) * nel;
@@ -455,7 +489,6 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         const size_t cb = (size_t)p->tcs_nchunks * tc_synth_chunk_bytes(spin);
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tcs_B, cb));
         bytes += cb;
-        p->tca_nchunk = (T + (spin ? 16 : 32) - 1) / (spin ? 16 : 32);
         const size_t bt = (size_t)M * p->tca_nchunk * kTcaBStage;
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_tca_B, bt));
         bytes += bt;

@@ -13,21 +13,24 @@
 // Work: one item per (order m, block of 128 degrees); items are ordered by m so that the
 // CTAs working at one time share the orders' ring data in L2.  A persistent CTA per SM
 // runs four roles that meet only at mbarriers:
-//   producer warps (one stage each, round robin): thread = (ring, recursion); start from
-//     the plan's recursion state at the block's first degree (FP64, the same arithmetic as
-//     the FP64 kernels), run the block's 128 steps, round mu to FP32, split it into three
+//   producer warps (one stage each, round robin): thread = (ring, recursion); four
+//     independent chains per thread, one per 32-degree segment of the block, each started
+//     from the plan's recursion state at its first degree (FP64, the same arithmetic as
+//     the FP64 kernels), run the segment's 32 steps, round mu to FP32, split it into three
 //     BF16 parts and store them as the A operand in MN-major layout (8 consecutive degrees
 //     per 16-byte store);
 //   a loader warp: one bulk copy per stage of the chunk's BF16x3 ring-data tiles (B
 //     operand, K-major), prepared once per launch by adj_prep_kernel from the FP64 ring
 //     spectra;
-//   one MMA warp: six split products per GEMM (hh, hm, mh, hl, lh, mm), hh into a
-//     double-buffered FP32 accumulator, the five smaller ones into a correction accumulator
-//     that runs over the whole item (relative size <= 2^-8);
+//   one MMA warp: six split products per GEMM (hh, hm, mh, hl, lh, mm) in four MMAs: hh
+//     (N = 64) into a double-buffered FP32 accumulator; the five smaller ones into a
+//     correction pair [X | Y] that runs over the whole item (relative size <= 2^-8), two
+//     of them with N = 128 over consecutive ring-data splits (h [m | l] and m [h | m]) so
+//     each A split is read from shared memory fewer times, and l h into X;
 //   four epilogue warps (thread = degree = tensor-memory lane): every 256 rings they fold
 //     the hh block sums, already combined into the half-grid sums, into FP64 accumulators
-//     in shared memory (FP32 rounding acts on <= 256 rings); at the item's end they add
-//     the correction sums, scale by c_l and write the item's a_lm (E, B for spin 2).
+//     in registers (FP32 rounding acts on <= 256 rings); at the item's end they add the
+//     correction sums X + Y, scale by c_l and write the item's a_lm (E, B for spin 2).
 // The item covers every ring, so no partial sums leave the chip and the result does not
 // depend on the order of the work.  Every wait is bounded (poll count and the plan's
 // watchdog time); on timeout the kernel records an error, every role leaves its loops,
@@ -48,9 +51,16 @@ using namespace tc;
 constexpr int kLB = kTcaLB;               // degrees per item = MMA M
 constexpr int kTK = 16;                   // rings per MMA = K
 constexpr int kN = 4 * kTcaMaps;          // 64 columns per GEMM = MMA N
-constexpr int kNP = 5;                    // producer warps
-constexpr int kNSA = 6;                   // A stages
+#ifndef JHTB_TCA_NP
+#define JHTB_TCA_NP 6
+#endif
+#ifndef JHTB_TCA_NSA
+#define JHTB_TCA_NSA 7
+#endif
+constexpr int kNP = JHTB_TCA_NP;          // producer warps
+constexpr int kNSA = JHTB_TCA_NSA;        // A stages
 constexpr int kNSB = 4;                   // B stages
+constexpr int kPrefetch = 8;              // ring-data tiles prefetched into L2 ahead of their copy
 constexpr int kATile = kLB * kTK * 2;     // one split of one A sub-tile: 4096 bytes
 constexpr int kBTile = kN * kTK * 2;      // one split of one B sub-tile: 2048 bytes
 constexpr int kAStage = 2 * 3 * kATile;   // 24 KB
@@ -61,11 +71,11 @@ constexpr int kThreads = (kNP + 6) * 32;
 
 template <int SPIN>
 struct AdjCfg {
-    static constexpr int NREC = SPIN ? 2 : 1;
     static constexpr int CR = SPIN ? 16 : 32;      // rings per stage
     static constexpr int NACC = SPIN ? 64 : 32;    // FP64 sums per degree: (p2, m2) or b, per map
     static constexpr int NG = SPIN ? 2 : 1;        // accumulators (GEMMs)
-    static constexpr int COL_CORR = 2 * NG * kN;   // hh buffers first: (buf * NG + g) * kN
+    static constexpr int COL_CORR = 2 * NG * kN;   // hh buffers first: (buf * NG + g) * kN, then the
+                                                   // correction pair [X | Y] of GEMM g at COL_CORR + 2 g kN
     static constexpr uint32_t TCOLS = SPIN ? 512 : 256;
 };
 
@@ -89,7 +99,7 @@ struct AdjParams {
     const double *cnorm;
     const TcaItem *items;
     int nitems;
-    const double2 *bst;     // block-start states [blk][nrec][T]
+    const double2 *bst;     // segment-start states, rows [block][chunk - cl][segment][lane]
     const short *bsc;
     const unsigned char *Bt;  // ring-data tiles [M][nchunk][kBStage]
     int nchunk;
@@ -99,9 +109,12 @@ struct AdjParams {
     int fold;               // stages per FP32 accumulation block
 };
 
-// kind::f16 instruction descriptor: FP32 accumulate, BF16 A (MN-major) and B (K-major).
-constexpr uint32_t kIdescAdj = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(kN >> 3) << 17) |
-                               ((uint32_t)(kLB >> 4) << 24);
+// kind::f16 instruction descriptors: FP32 accumulate, BF16 A (MN-major) and B (K-major),
+// M = 128, N = 64 (one split of the ring data) or 128 (two consecutive splits).
+constexpr uint32_t idesc_adj(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kLB >> 4) << 24);
+}
+constexpr uint32_t kIdescAdj = idesc_adj(kN), kIdescAdj2 = idesc_adj(2 * kN);
 // A sub-tile, MN-major without swizzle: 8 degrees x 8 rings core matrices of 128 bytes,
 // degree groups 128 bytes apart (SBO), the two 8-ring halves 2048 bytes apart (LBO).
 constexpr uint32_t kALbo = 2048, kASbo = 128;
@@ -118,74 +131,78 @@ __device__ __forceinline__ void adj_fail(int *f, int *err) {
 __device__ __forceinline__ int item_stages(const TcaItem &q) { return q.c1 > q.c0 ? q.c1 - q.c0 : 0; }
 
 // ---------------------------------------------------------------------------------
-// producers: 128 recursion steps per (ring, recursion) -> split A operand
+// producers: four 32-degree recursion chains per (ring, recursion) -> split A operand
 // ---------------------------------------------------------------------------------
-template <int SPIN, bool SLOW>
-__device__ __forceinline__ void adj_block_steps(const double2 *coef, int i0, int nst, int h, double x, double &u1,
-                                                double &u2, int &sc, unsigned char *As, int j, int k) {
-    const double gsg = h ? -1.0 : 1.0;
+constexpr int kSeg = kTcaSeg;        // chains per thread: the block's 32-degree segments
+constexpr int kSegLen = kLB / kSeg;  // steps per chain
+
+// One stage of one lane: chain c runs the steps of degrees [32 c, 32 c + 32) of the block
+// from its stored segment state; the four chains are independent, so their FP64 steps
+// overlap.  Values of a chain in the underflow range (scale exponent < 0) are zero; such a
+// chain is rescaled once per 8 steps (8 steps grow a value by far less than the 2^800 of
+// headroom above the threshold, so this matches the per-step check of the FP64 kernels in
+// every value that reaches FP32).  TAIL: the block runs past lmax (nrem < 128 degrees
+// exist); the missing rows are zero.
+template <bool TAIL>
+__device__ __forceinline__ void adj_stage(const double2 *coef, int nrem, double x, double (&u1)[kSeg],
+                                          double (&u2)[kSeg], int (&sc)[kSeg], unsigned char *As, int j, int k) {
+    bool low[kSeg];
+#pragma unroll
+    for (int c = 0; c < kSeg; ++c) low[c] = __any_sync(0xffffffffu, sc[c] != 0);
 #pragma unroll 1
-    for (int g8 = 0; g8 < kLB / 8; ++g8) {
-        const int ib = i0 + g8 * 8;
-        uint32_t pk[3][4];
-        if (ib + 8 <= nst) {
-            double t[8];
+    for (int g = 0; g < kSegLen / 8; ++g) {
+        double v[kSeg][8];
+#pragma unroll
+        for (int c = 0; c < kSeg; ++c) {
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const double2 c = coef[g8 * 8 + q];
-                t[q] = SPIN ? fma(c.x, x, gsg * c.y) : c.x * x;
+                const double2 cf = coef[c * kSegLen + g * 8 + q];
+                const double u = fma(fma(cf.x, x, cf.y), u1[c], -u2[c]);
+                u2[c] = u1[c];
+                u1[c] = u;
+                v[c][q] = u;
             }
-            double v[8];
+        }
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                double u = fma(t[q], u1, -u2);
-                double prev = u1;
-                if (SLOW) rescale(u, prev, sc);
-                u2 = prev;
-                u1 = u;
-                v[q] = (SLOW && sc != 0) ? 0.0 : u;
-            }
-            split3_pack8(v, pk);
-        } else {
-            // the block's tail past lmax: zero rows (their outputs are not written)
-            double vt[8];
+        for (int c = 0; c < kSeg; ++c) {
+            if (low[c] && sc[c] != 0) {
 #pragma unroll
-            for (int q = 0; q < 8; q += 2) {
-                double *v = vt + q;
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int i = ib + q + e;
-                    double val = 0.0;
-                    if (i < nst) {
-                        const double2 c = coef[g8 * 8 + q + e];
-                        const double tt = SPIN ? fma(c.x, x, gsg * c.y) : c.x * x;
-                        double u = fma(tt, u1, -u2);
-                        double prev = u1;
-                        rescale(u, prev, sc);
-                        u2 = prev;
-                        u1 = u;
-                        val = sc != 0 ? 0.0 : u;
-                    }
-                    v[e] = val;
+                for (int q = 0; q < 8; ++q) v[c][q] = 0.0;
+                if (fabs(u1[c]) > kBig) {
+                    u1[c] *= kScaleDown;
+                    u2[c] *= kScaleDown;
+                    sc[c] += 1;
                 }
             }
-            split3_pack8(vt, pk);
-        }
-        const uint32_t off = amn_off(g8, k);
+            if (TAIL) {
 #pragma unroll
-        for (int sp = 0; sp < 3; ++sp) {
-            uint4 w = make_uint4(pk[sp][0], pk[sp][1], pk[sp][2], pk[sp][3]);
-            *reinterpret_cast<uint4 *>(As + j * 3 * kATile + sp * kATile + off) = w;
+                for (int q = 0; q < 8; ++q)
+                    if (c * kSegLen + g * 8 + q >= nrem) v[c][q] = 0.0;
+            }
+            uint32_t pk[3][4];
+            split3_pack8(v[c], pk);
+            const uint32_t off = amn_off(c * (kSegLen / 8) + g, k);
+#pragma unroll
+            for (int sp = 0; sp < 3; ++sp) {
+                const uint4 w = make_uint4(pk[sp][0], pk[sp][1], pk[sp][2], pk[sp][3]);
+                *reinterpret_cast<uint4 *>(As + j * 3 * kATile + sp * kATile + off) = w;
+            }
         }
     }
 }
 
+// Lane = (j, k): spin 2 runs recursion h = j (+2 for sub-tile 0, -2 for sub-tile 1) on ring
+// k of the 16-ring chunk; spin 0 runs ring 16 j + k of the 32-ring chunk.  The -2
+// recursion t_l = alpha_l x - gamma_l runs as w_i = (-1)^i mu_i (i = degree offset in the
+// block): w_i = (alpha_i (-x) + gamma_i) w_{i-1} - w_{i-2}, the same arithmetic as the +2
+// recursion with x negated and the first state value negated, without a multiply per step;
+// the epilogue restores the sign (-1)^i of the row.
 template <int SPIN>
 __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int lane) {
     using C = AdjCfg<SPIN>;
     const int j = lane >> 4, k = lane & 15;
-    const int h = SPIN ? j : 0;  // recursion (spin 2: +2 for sub-tile 0, -2 for sub-tile 1)
-    unsigned gc = 0, n = 0;      // stages and items of this CTA so far
+    const bool neg = SPIN && j == 1;
+    unsigned gc = 0, n = 0;  // stages and items of this CTA so far
     bool ok = true;
     for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x, ++n) {
         if (adj_failed(&sm.fail)) break;
@@ -194,35 +211,50 @@ __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int l
         const int lmin = __ldg(&p.seed[q.m].lmin);
         const int nst = p.lmax - lmin + 1;
         const int i0 = q.lb * kLB;
+        const int nrem = nst - i0;
         const int cb = n & 1;
         if (!mbar_wait_warp(&sm.coefFull[cb], (n >> 1) & 1u, p.wait_ns)) {
             ok = false;
             break;
         }
-        // start state of this (ring, recursion) at the block's first degree for stage s, loaded
-        // one stage of this warp ahead so the memory latency overlaps the previous stage
-        auto load_state = [&](int s, double &x, double &u1, double &u2, int &sc) {
+        // segment states of this lane for stage s, loaded one stage of this warp ahead so the
+        // memory latency overlaps the previous stage
+        auto load_state = [&](int s, double &x, double (&u1)[kSeg], double (&u2)[kSeg], int (&sc)[kSeg]) {
             const int c = q.c0 + s;
-            const int t = SPIN ? c * C::CR + k : c * C::CR + j * 16 + k;
-            x = u1 = u2 = 0.0;
-            sc = 0;
+            const int t = SPIN ? c * C::CR + k : c * C::CR + lane;
+            x = 0.0;
+#pragma unroll
+            for (int g = 0; g < kSeg; ++g) {
+                u1[g] = u2[g] = 0.0;
+                sc[g] = 0;
+            }
             if (s < nstg && t < p.T) {
-                const size_t e = ((size_t)q.blk * C::NREC + h) * p.T + t;
-                const double2 st = p.bst[e];
                 x = __ldg(&p.x[t]);
-                u1 = st.x;
-                u2 = st.y;
-                sc = p.bsc[e];
+                if (neg) x = -x;
+                const long long row = q.soff + (long long)(c - q.cl) * (kSeg * 32) + lane;
+#pragma unroll
+                for (int g = 0; g < kSeg; ++g) {
+                    const double2 st = p.bst[row + g * 32];
+                    u1[g] = neg ? -st.x : st.x;
+                    u2[g] = st.y;
+                    sc[g] = p.bsc[row + g * 32];
+                }
             }
         };
-        double xn, u1n, u2n;
-        int scn;
+        double xn, u1n[kSeg], u2n[kSeg];
+        int scn[kSeg];
         load_state(w, xn, u1n, u2n, scn);
         for (int s = w; s < nstg; s += kNP) {
             const unsigned g = gc + (unsigned)s;
             const int sA = g % kNSA;
-            double x = xn, u1 = u1n, u2 = u2n;
-            int sc = scn;
+            double x = xn, u1[kSeg], u2[kSeg];
+            int sc[kSeg];
+#pragma unroll
+            for (int c = 0; c < kSeg; ++c) {
+                u1[c] = u1n[c];
+                u2[c] = u2n[c];
+                sc[c] = scn[c];
+            }
             load_state(s + kNP, xn, u1n, u2n, scn);
             if (g >= (unsigned)kNSA && !mbar_wait_warp(&sm.emptyA[sA], ((g / kNSA) - 1u) & 1u, p.wait_ns)) {
                 ok = false;
@@ -230,10 +262,10 @@ __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int l
             }
             tc_fence_after();  // the stage's previous MMAs are complete before it is overwritten
             unsigned char *As = sm.A[sA];
-            if (__all_sync(0xffffffffu, sc == 0))
-                adj_block_steps<SPIN, false>(sm.coef[cb], i0, nst, h, x, u1, u2, sc, As, j, k);
+            if (nrem >= kLB)
+                adj_stage<false>(sm.coef[cb], nrem, x, u1, u2, sc, As, j, k);
             else
-                adj_block_steps<SPIN, true>(sm.coef[cb], i0, nst, h, x, u1, u2, sc, As, j, k);
+                adj_stage<true>(sm.coef[cb], nrem, x, u1, u2, sc, As, j, k);
             fence_async_smem();
             __syncwarp();
             if (lane == 0) mbar_arrive(&sm.fullA[sA]);
@@ -252,42 +284,47 @@ __device__ void adj_producer(const AdjParams &p, AdjSmem<SPIN> &sm, int w, int l
 // ---------------------------------------------------------------------------------
 template <int SPIN>
 __device__ void adj_loader(const AdjParams &p, AdjSmem<SPIN> &sm, int lane) {
-    unsigned gc = 0, n = 0;
-    bool ok = true;
     if (p.inject == kInjectStall) return;  // test hook: no stage is ever published
-    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x, ++n) {
-        if (adj_failed(&sm.fail)) break;
-        const TcaItem q = p.items[it];
-        const int nstg = item_stages(q);
-        const int cb = n & 1;
-        if (n >= 2 && !mbar_wait_warp(&sm.coefEmpty[cb], ((n >> 1) - 1u) & 1u, p.wait_ns)) {
-            ok = false;
-            break;
-        }
-        if (lane == 0) {
+    if (lane == 0) {  // one thread issues every copy
+        unsigned n = 0;
+        int sB = 0;
+        uint32_t phB = 0;  // parity of the current round of B stages
+        bool ok = true, first = true;
+        for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x, ++n) {
+            if (*(volatile int *)&sm.fail) break;
+            const TcaItem q = p.items[it];
+            const int nstg = item_stages(q);
+            const int cb = n & 1;
+            const unsigned char *tiles = p.Bt + ((size_t)q.m * p.nchunk + q.c0) * kBStage;
+            for (int s = 0; s < min(kPrefetch, nstg); ++s) bulk_prefetch_l2(tiles + (size_t)s * kBStage, kBStage);
+            if (n >= 2 && !mbar_wait(&sm.coefEmpty[cb], ((n >> 1) - 1u) & 1u, p.wait_ns)) {
+                ok = false;
+                break;
+            }
             const int lmin = __ldg(&p.seed[q.m].lmin);
             const int i0 = q.lb * kLB;
             const uint32_t bytes = (uint32_t)min(kLB, p.lmax - lmin + 1 - i0) * 16u;
             mbar_arrive_tx(&sm.coefFull[cb], bytes);
             bulk_g2s(sm.coef[cb], p.ag + alm_index(lmin, q.m, p.lmax) + i0, bytes, &sm.coefFull[cb]);
-        }
-        __syncwarp();
-        for (int s = 0; s < nstg; ++s) {
-            const unsigned g = gc + (unsigned)s;
-            const int sB = g % kNSB;
-            if (g >= (unsigned)kNSB && !mbar_wait_warp(&sm.emptyB[sB], ((g / kNSB) - 1u) & 1u, p.wait_ns)) {
-                ok = false;
-                break;
-            }
-            if (lane == 0) {
+            for (int s = 0; s < nstg; ++s) {
+                // the stage's previous round has been consumed (the first round starts free)
+                if (!first && !mbar_wait(&sm.emptyB[sB], phB ^ 1u, p.wait_ns)) {
+                    ok = false;
+                    break;
+                }
+                if (s + kPrefetch < nstg) bulk_prefetch_l2(tiles + (size_t)(s + kPrefetch) * kBStage, kBStage);
                 mbar_arrive_tx(&sm.fullB[sB], kBStage);
-                bulk_g2s(sm.B[sB], p.Bt + ((size_t)q.m * p.nchunk + (q.c0 + s)) * kBStage, kBStage, &sm.fullB[sB]);
+                bulk_g2s(sm.B[sB], tiles + (size_t)s * kBStage, kBStage, &sm.fullB[sB]);
+                if (++sB == kNSB) {
+                    sB = 0;
+                    phB ^= 1u;
+                    first = false;
+                }
             }
-            __syncwarp();
         }
-        gc += (unsigned)nstg;
+        if (!ok) adj_fail(&sm.fail, p.err);
     }
-    if (!ok) adj_fail(&sm.fail, p.err);
+    __syncwarp();
 }
 
 // ---------------------------------------------------------------------------------
@@ -296,64 +333,71 @@ __device__ void adj_loader(const AdjParams &p, AdjSmem<SPIN> &sm, int lane) {
 template <int SPIN>
 __device__ void adj_mma(const AdjParams &p, AdjSmem<SPIN> &sm, uint32_t tbase, int lane) {
     using C = AdjCfg<SPIN>;
-    unsigned gc = 0, bk = 0, ncorr = 0;
-    bool ok = true;
-    for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
-        if (adj_failed(&sm.fail)) break;
-        const TcaItem q = p.items[it];
-        const int nstg = item_stages(q);
-        for (int s = 0; s < nstg; ++s) {
-            const unsigned g = gc + (unsigned)s;
-            const int sA = g % kNSA, sB = g % kNSB;
-            const bool bstart = (s % p.fold) == 0;
-            const bool bend = (s % p.fold) == p.fold - 1 || s == nstg - 1;
-            const unsigned kb = bk & 1u;
-            if (!mbar_wait_warp(&sm.fullA[sA], (g / kNSA) & 1u, p.wait_ns) ||
-                !mbar_wait_warp(&sm.fullB[sB], (g / kNSB) & 1u, p.wait_ns) ||
-                (bstart && bk >= 2 && !mbar_wait_warp(&sm.accEmpty[kb], ((bk >> 1) - 1u) & 1u, p.wait_ns)) ||
-                (s == 0 && ncorr > 0 && !mbar_wait_warp(&sm.corrEmpty, (ncorr - 1u) & 1u, p.wait_ns))) {
-                ok = false;
-                break;
-            }
-            tc_fence_after();
-            if (lane == 0) {
+    if (lane == 0) {  // one thread waits and issues; stage indices and parities are counters
+        unsigned bk = 0, ncorr = 0;
+        int sA = 0, sB = 0;
+        uint32_t phA = 0, phB = 0;
+        bool ok = true;
+        const uint64_t dA0 = smem_desc(sm.A[0], kALbo, kASbo), dB0 = smem_desc(sm.B[0], 128, 256);
+        for (int it = blockIdx.x; it < p.nitems && ok; it += gridDim.x) {
+            if (*(volatile int *)&sm.fail) break;
+            const TcaItem q = p.items[it];
+            const int nstg = item_stages(q);
+            int fcount = 0;  // stages of the current FP32 accumulation block so far
+            for (int s = 0; s < nstg; ++s) {
+                const bool bstart = fcount == 0;
+                const bool bend = fcount == p.fold - 1 || s == nstg - 1;
+                const unsigned kb = bk & 1u;
+                if (!mbar_wait(&sm.fullB[sB], phB, p.wait_ns) || !mbar_wait(&sm.fullA[sA], phA, p.wait_ns) ||
+                    (bstart && bk >= 2 && !mbar_wait(&sm.accEmpty[kb], ((bk >> 1) - 1u) & 1u, p.wait_ns)) ||
+                    (s == 0 && ncorr > 0 && !mbar_wait(&sm.corrEmpty, (ncorr - 1u) & 1u, p.wait_ns))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
 #pragma unroll
                 for (int jj = 0; jj < 2; ++jj) {
                     const int gg = SPIN ? jj : 0;  // accumulator of this sub-tile
                     const uint32_t dh = tbase + (uint32_t)((kb * C::NG + gg) * kN);
-                    const uint32_t dc = tbase + (uint32_t)(C::COL_CORR + gg * kN);
-                    const unsigned char *Aj = sm.A[sA] + jj * 3 * kATile;
-                    const unsigned char *Bj = sm.B[sB] + jj * 3 * kBTile;
-                    const uint64_t a0 = smem_desc(Aj, kALbo, kASbo), a1 = smem_desc(Aj + kATile, kALbo, kASbo),
-                                   a2 = smem_desc(Aj + 2 * kATile, kALbo, kASbo);
-                    const uint64_t c0 = smem_desc(Bj, 128, 256), c1 = smem_desc(Bj + kBTile, 128, 256),
-                                   c2 = smem_desc(Bj + 2 * kBTile, 128, 256);
+                    const uint32_t dc = tbase + (uint32_t)(C::COL_CORR + gg * 2 * kN);
+                    // descriptors: the address field (bits 0-13, bytes / 16) advanced from the
+                    // first stage's; shared-memory offsets stay far below 2^18 bytes
+                    const uint64_t a0 = dA0 + (uint64_t)((sA * kAStage + jj * 3 * kATile) >> 4);
+                    const uint64_t a1 = a0 + (kATile >> 4), a2 = a0 + (2 * kATile >> 4);
+                    const uint64_t c0 = dB0 + (uint64_t)((sB * kBStage + jj * 3 * kBTile) >> 4);
+                    const uint64_t c1 = c0 + (kBTile >> 4);
                     // first write of each accumulator starts it at zero
                     const uint32_t acc_h = (bstart && (SPIN || jj == 0)) ? 0u : 1u;
                     const uint32_t acc_c = (s == 0 && (SPIN || jj == 0)) ? 0u : 1u;
-                    umma_f16_ss(dh, a0, c0, kIdescAdj, acc_h);  // hh
-                    umma_f16_ss(dc, a0, c1, kIdescAdj, acc_c);  // hm
-                    umma_f16_ss(dc, a1, c0, kIdescAdj, 1u);     // mh
-                    umma_f16_ss(dc, a0, c2, kIdescAdj, 1u);     // hl
-                    umma_f16_ss(dc, a2, c0, kIdescAdj, 1u);     // lh
-                    umma_f16_ss(dc, a1, c1, kIdescAdj, 1u);     // mm
+                    umma_f16_ss(dh, a0, c0, kIdescAdj, acc_h);   // hh
+                    umma_f16_ss(dc, a0, c1, kIdescAdj2, acc_c);  // [hm | hl]: B = [m | l] splits
+                    umma_f16_ss(dc, a1, c0, kIdescAdj2, 1u);     // [mh | mm]: B = [h | m] splits
+                    umma_f16_ss(dc, a2, c0, kIdescAdj, 1u);      // lh into the first half
                 }
                 umma_commit(&sm.emptyA[sA]);
                 umma_commit(&sm.emptyB[sB]);
                 if (bend) umma_commit(&sm.accFull[kb]);
+                if (++sA == kNSA) {
+                    sA = 0;
+                    phA ^= 1u;
+                }
+                if (++sB == kNSB) {
+                    sB = 0;
+                    phB ^= 1u;
+                }
+                if (bend) {
+                    ++bk;
+                    fcount = 0;
+                } else {
+                    ++fcount;
+                }
             }
-            __syncwarp();
-            if (bend) ++bk;
+            if (nstg > 0) ++ncorr;
         }
-        if (!ok) break;
-        if (nstg > 0) ++ncorr;
-        gc += (unsigned)nstg;
-    }
-    if (!ok) adj_fail(&sm.fail, p.err);
-    // every issued MMA has completed before tensor memory is released
-    if (lane == 0) {
+        if (!ok) adj_fail(&sm.fail, p.err);
+        // every issued MMA has completed before tensor memory is released
         umma_commit(&sm.fin);
-        if (!mbar_wait(&sm.fin, 0u, p.wait_ns)) adj_fail(&sm.fail, p.err);  // lane 0 alone
+        if (!mbar_wait(&sm.fin, 0u, p.wait_ns)) adj_fail(&sm.fail, p.err);
     }
     __syncwarp();
 }
@@ -377,11 +421,12 @@ __device__ __forceinline__ void adj_fold(double (&acc)[AdjCfg<SPIN>::NACC], uint
             for (int e = 0; e < 2; ++e) {  // two maps of 4 columns each
                 const int b = col / 4 + e;
                 const float *P = vp + 4 * e, *Mv = vm + 4 * e;
-                // p2 = D+[Vpn] + s D-[Sp],  m2 = D-[Vmn] + s D+[Sm]
-                acc[4 * b + 0] += (double)P[0] + (double)(sgn * Mv[2]);
-                acc[4 * b + 1] += (double)P[1] + (double)(sgn * Mv[3]);
-                acc[4 * b + 2] += (double)Mv[0] + (double)(sgn * P[2]);
-                acc[4 * b + 3] += (double)Mv[1] + (double)(sgn * P[3]);
+                // p2 = D+[Vpn] + s D-[Sp],  m2 = D-[Vmn] + s D+[Sm], where the accumulator
+                // holds s D- (the producers' sign substitution), s = (-1)^row
+                acc[4 * b + 0] += (double)P[0] + (double)Mv[2];
+                acc[4 * b + 1] += (double)P[1] + (double)Mv[3];
+                acc[4 * b + 2] += (double)sgn * ((double)Mv[0] + (double)P[2]);
+                acc[4 * b + 3] += (double)sgn * ((double)Mv[1] + (double)P[3]);
             }
         } else {
 #pragma unroll
@@ -425,9 +470,10 @@ __device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__r
             const uint32_t hP = tl + (uint32_t)((kb * C::NG + 0) * kN);
             const uint32_t hM = tl + (uint32_t)((kb * C::NG + (SPIN ? 1 : 0)) * kN);
             adj_fold<SPIN>(acc, hP, hM, sgn);
-            if (fb == nfb - 1) {  // the item's correction sums
-                const uint32_t cP = tl + (uint32_t)C::COL_CORR, cM = tl + (uint32_t)(C::COL_CORR + (SPIN ? kN : 0));
+            if (fb == nfb - 1) {  // the item's correction sums: both halves [X | Y] of each GEMM
+                const uint32_t cP = tl + (uint32_t)C::COL_CORR, cM = tl + (uint32_t)(C::COL_CORR + (SPIN ? 2 * kN : 0));
                 adj_fold<SPIN>(acc, cP, cM, sgn);
+                adj_fold<SPIN>(acc, cP + kN, cM + kN, sgn);
             }
             tc_fence_before();
             __syncwarp();
@@ -578,19 +624,22 @@ __global__ void __launch_bounds__(256) adj_prep_kernel(int lmax, int T, int nrin
 }
 
 // ---------------------------------------------------------------------------------
-// plan creation: the recursion state at the start of every 128-degree block, every ring
+// plan creation: the recursion state at the start of every 32-degree segment of every
+// 128-degree block, for the rings of the block's live chunks (the producer lane layout)
 // ---------------------------------------------------------------------------------
 template <int SPIN>
-__global__ void __launch_bounds__(128) tca_block_state_kernel(int lmax, int T, const double *__restrict__ x,
-                                                              const double *__restrict__ logsin,
-                                                              const double *__restrict__ logch,
-                                                              const double *__restrict__ logsh,
-                                                              const SeedParam *__restrict__ seed,
-                                                              const double *__restrict__ alpha,
-                                                              const double *__restrict__ gamma,
-                                                              const int *__restrict__ blk_off, double2 *__restrict__ bst,
-                                                              short *__restrict__ bsc) {
-    constexpr int NREC = SPIN ? 2 : 1;
+__global__ void __launch_bounds__(128) tca_segment_state_kernel(int lmax, int T, const double *__restrict__ x,
+                                                                const double *__restrict__ logsin,
+                                                                const double *__restrict__ logch,
+                                                                const double *__restrict__ logsh,
+                                                                const SeedParam *__restrict__ seed,
+                                                                const double *__restrict__ alpha,
+                                                                const double *__restrict__ gamma,
+                                                                const int *__restrict__ blk_off,
+                                                                const int *__restrict__ blk_cl,
+                                                                const long long *__restrict__ blk_soff,
+                                                                double2 *__restrict__ bst, short *__restrict__ bsc) {
+    constexpr int CR = SPIN ? 16 : 32;
     const int t = blockIdx.x * 128 + threadIdx.x;
     const int h = blockIdx.y, m = blockIdx.z;
     if (t >= T) return;
@@ -604,19 +653,28 @@ __global__ void __launch_bounds__(128) tca_block_state_kernel(int lmax, int T, c
     make_seed(lg, sd.sign[h], mant, sc);
     double u1 = 0.0, u2 = -mant;
     const double gsg = h ? -1.0 : 1.0;
+    const int c = t / CR;
+    const int lane = SPIN ? h * 16 + (t & 15) : (t & 31);
     const int nblk = (nst + kLB - 1) / kLB;
     for (int lb = 0; lb < nblk; ++lb) {
-        const size_t e = ((size_t)(blk_off[m] + lb) * NREC + h) * T + t;
-        bst[e] = make_double2(u1, u2);
-        bsc[e] = (short)max(sc, -32768);
-        const int i1 = min(nst, (lb + 1) * kLB);
-        for (int i = lb * kLB; i < i1; ++i) {
-            const double tt = fma(alpha[b0 + i], xt, SPIN ? gsg * gamma[b0 + i] : 0.0);
-            double u = fma(tt, u1, -u2);
-            double prev = u1;
-            rescale(u, prev, sc);
-            u2 = prev;
-            u1 = u;
+        const int blk = blk_off[m] + lb;
+        const int cl = blk_cl[blk];
+        const long long row = blk_soff[blk] + (long long)(c - cl) * (kTcaSeg * 32) + lane;
+        for (int g = 0; g < kTcaSeg; ++g) {
+            const int i0 = lb * kLB + g * (kLB / kTcaSeg);
+            if (c >= cl) {
+                bst[row + g * 32] = i0 < nst ? make_double2(u1, u2) : make_double2(0.0, 0.0);
+                bsc[row + g * 32] = i0 < nst ? (short)max(sc, -32768) : (short)0;
+            }
+            const int i1 = min(nst, i0 + kLB / kTcaSeg);
+            for (int i = i0; i < i1; ++i) {
+                const double tt = fma(alpha[b0 + i], xt, SPIN ? gsg * gamma[b0 + i] : 0.0);
+                double u = fma(tt, u1, -u2);
+                double prev = u1;
+                rescale(u, prev, sc);
+                u2 = prev;
+                u1 = u;
+            }
         }
     }
 }
@@ -626,11 +684,13 @@ __global__ void __launch_bounds__(128) tca_block_state_kernel(int lmax, int T, c
 int launch_tca_block_states(const Plan &p, cudaStream_t s) {
     const dim3 grid((p.T + 127) / 128, p.spin ? 2 : 1, p.M);
     if (p.spin)
-        tca_block_state_kernel<2><<<grid, 128, 0, s>>>(p.lmax, p.T, p.d_x, p.d_logsin, p.d_logch, p.d_logsh, p.d_seed,
-                                                        p.d_alpha, p.d_gamma, p.d_tca_blk_off, p.d_tca_st, p.d_tca_sc);
+        tca_segment_state_kernel<2><<<grid, 128, 0, s>>>(p.lmax, p.T, p.d_x, p.d_logsin, p.d_logch, p.d_logsh, p.d_seed,
+                                                          p.d_alpha, p.d_gamma, p.d_tca_blk_off, p.d_tca_blk_cl,
+                                                          p.d_tca_blk_soff, p.d_tca_st, p.d_tca_sc);
     else
-        tca_block_state_kernel<0><<<grid, 128, 0, s>>>(p.lmax, p.T, p.d_x, p.d_logsin, p.d_logch, p.d_logsh, p.d_seed,
-                                                        p.d_alpha, p.d_gamma, p.d_tca_blk_off, p.d_tca_st, p.d_tca_sc);
+        tca_segment_state_kernel<0><<<grid, 128, 0, s>>>(p.lmax, p.T, p.d_x, p.d_logsin, p.d_logch, p.d_logsh, p.d_seed,
+                                                          p.d_alpha, p.d_gamma, p.d_tca_blk_off, p.d_tca_blk_cl,
+                                                          p.d_tca_blk_soff, p.d_tca_st, p.d_tca_sc);
     JHTB_CUDA_TRY(cudaGetLastError());
     return JHTB_OK;
 }

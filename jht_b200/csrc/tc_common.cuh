@@ -44,18 +44,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// The same test, but a thread whose phase is not complete is suspended until it completes
+// or about hint_ns nanoseconds pass: a waiting warp takes no issue slots from the others.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+constexpr uint32_t kSuspendNs = 20000;  // longest suspension per poll (the watchdog checks between polls)
 __device__ __forceinline__ uint64_t globaltimer_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
 }
 // Bounded wait: at most kWaitLimit polls and limit_ns of %globaltimer time; returns false
-// on timeout (the caller records the error and leaves its loop).
+// on timeout (the caller records the error and leaves its loop).  After a first plain test
+// the thread sleeps in the barrier between polls.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;  // the common case: no timer read
     const uint64_t t0 = globaltimer_ns();
     for (unsigned it = 0; it < kWaitLimit; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 63u) == 63u && globaltimer_ns() - t0 > limit_ns) return false;
+        if (mbar_try_wait_sleep(bar, parity, kSuspendNs)) return true;
+        if (globaltimer_ns() - t0 > limit_ns) return false;
     }
     return false;
 }
@@ -149,28 +163,32 @@ __device__ __forceinline__ void rescale(double &u, double &prev, int &sc) {
     }
 }
 
+// Two FP32 values rounded to BF16 (nearest, ties to even) and packed: lo in the low half.
+__device__ __forceinline__ uint32_t cvt_bf16x2(float hi, float lo) {
+    uint32_t d;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
 // Eight values: the eight FP64 -> FP32 conversions are issued back to back (they run on
 // a variable-latency unit, so issuing them together overlaps their latencies), then each
-// consecutive pair is split and packed as in split3_pair: pk[part][pair].
+// consecutive pair is split with paired conversions: h = bf16(x), m = bf16(x - h),
+// l = x - h - m (exact: at most 8 significant bits remain), packed pk[part][pair] with the
+// even value in the low half.
 __device__ __forceinline__ void split3_pack8(const double (&v)[8], uint32_t (&pk)[3][4]) {
     float f[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) f[i] = (float)v[i];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        uint32_t h[2], m[2], l[2];
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const float x = f[2 * q + e];
-            h[e] = bf16_rn_bits(x);
-            const float r1 = x - __uint_as_float(h[e]);
-            m[e] = bf16_rn_bits(r1);
-            const float r2 = r1 - __uint_as_float(m[e]);
-            l[e] = __float_as_uint(r2) & 0xFFFF0000u;
-        }
-        pk[0][q] = __byte_perm(h[0], h[1], 0x7632);
-        pk[1][q] = __byte_perm(m[0], m[1], 0x7632);
-        pk[2][q] = __byte_perm(l[0], l[1], 0x7632);
+        const float x0 = f[2 * q], x1 = f[2 * q + 1];
+        const uint32_t h = cvt_bf16x2(x1, x0);
+        const float r10 = x0 - __uint_as_float(h << 16), r11 = x1 - __uint_as_float(h & 0xFFFF0000u);
+        const uint32_t m = cvt_bf16x2(r11, r10);
+        const float r20 = r10 - __uint_as_float(m << 16), r21 = r11 - __uint_as_float(m & 0xFFFF0000u);
+        pk[0][q] = h;
+        pk[1][q] = m;
+        pk[2][q] = __byte_perm(__float_as_uint(r20), __float_as_uint(r21), 0x7632);
     }
 }
 
@@ -193,6 +211,10 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+// Prefetch of a global range into L2 (no shared-memory destination, no completion).
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 // mbar_wait by every lane of a warp, with one verdict for the warp: a lane that ran out
 // makes the whole warp leave together, so no warp-collective instruction after the wait
