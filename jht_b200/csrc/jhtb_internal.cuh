@@ -65,14 +65,17 @@ constexpr int kTwLen = 32768;    // twiddle table length: every FFT and split le
 constexpr int kFftPiece = 4096;  // largest FFT held in shared memory; longer ones run in pieces
 constexpr int kFftLogMax = 13;
 
-// Ring FFT modes.
-enum RingMode : int { kDirect = 0, kBluestein = 1 };
+// Ring FFT modes: kDirect (N a power of two), kBluestein (chirp-z of length N), kSplit4
+// (N = 4 i: four chirp-z transforms of length i and a radix-4 combination).
+enum RingMode : int { kDirect = 0, kBluestein = 1, kSplit4 = 2 };
+constexpr int kBigN = 8192;      // largest ring transform held whole in shared memory (large-ring kernel)
 
 struct RingDesc {
     int N;          // pixels in the ring
-    int mode;       // kDirect (N a power of two) or kBluestein
-    int P;          // FFT length: N (direct) or Bluestein length (power of two >= 2N-1)
-    int Q;          // pieces of P / Q <= kFftPiece points (1, 2, 4 or 8)
+    int mode;       // RingMode
+    int P;          // FFT length: N (direct), Bluestein length (power of two >= 2N-1), or for
+                    // kSplit4 the Bluestein length of the quarter ring (power of two >= N/2-1)
+    int Q;          // pieces of P / Q <= kFftPiece points (1, 2, 4 or 8) in the piecewise path
     long long start;   // first pixel
     long long bh_off;  // offset (complex units) of this length's chirp spectrum
     double phi0;       // azimuth of the first pixel
@@ -190,8 +193,12 @@ struct Plan {
     int ring_t0, ring_t1;
     int nsynth;           // entries of d_synth_order (items inside the range)
     int tc_norder;        // entries of d_tc_order
-    int *d_ring_list;     // [nring_list] ring indices of the range, or null for all rings
-    int nring_list;
+    // rings of the plan's range by kernel: ring_small (one 256-thread CTA per ring, pieces
+    // through global scratch above kFftPiece points) and ring_big (512 threads, the whole
+    // transform of up to kBigN points in shared memory)
+    int *d_ring_small, *d_ring_big;
+    int nring_small, nring_big;
+    std::vector<unsigned char> h_ring_big;  // [ring] 1 when the large-ring kernel takes it
     std::vector<int> h_lw, h_a_lw, h_tc_lw;  // start l per item, kept for re-sorting
 
     // workspace

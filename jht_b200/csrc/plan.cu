@@ -89,7 +89,7 @@ void free_plan(Plan *p) {
     void *ptrs[] = {p->d_x,     p->d_logsin, p->d_logch, p->d_logsh,   p->d_rings, p->d_tw,
                     p->d_bh,    p->d_seed,   p->d_alpha, p->d_gamma,   p->d_cnorm, p->d_F,
                     p->d_W,     p->d_W2,     p->d_scratch, p->d_lw, p->d_st, p->d_stsc, p->d_synth_order,
-                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err, p->d_ring_list};
+                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err, p->d_ring_small, p->d_ring_big};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (p->a_owns_tables) {
@@ -117,8 +117,10 @@ void free_plan(Plan *p) {
 // Cost-sorted item orders of the persistent kernels, restricted to the items whose
 // tile lies inside the plan's ring range, and the ring list of the azimuthal stage.
 // Called at plan creation and again whenever the range changes.
+int build_ring_lists(Plan *p, size_t &bytes);
+
 int build_orders(Plan *p) {
-    const int L = p->lmax, M = p->M, T = p->T;
+    const int L = p->lmax, M = p->M;
     const int t0 = p->ring_t0, t1 = p->ring_t1;
     size_t bytes = 0;
     auto refresh = [&](int **dptr, const std::vector<int> &h) -> int {
@@ -217,19 +219,30 @@ int build_orders(Plan *p) {
         p->d_tca_items = nullptr;
         if ((rc = upload(&p->d_tca_items, items, bytes))) return rc;
     }
-    // azimuthal stage: the range's northern rings and their southern mirrors
-    if (p->d_ring_list) cudaFree(p->d_ring_list);
-    p->d_ring_list = nullptr;
-    p->nring_list = 0;
-    if (t0 != 0 || t1 != T) {
-        std::vector<int> rl;
-        for (int t = t0; t < t1; ++t) {
-            rl.push_back(t);
-            if (t < T - 1) rl.push_back(p->nrings - 1 - t);
-        }
-        p->nring_list = (int)rl.size();
-        if ((rc = upload(&p->d_ring_list, rl, bytes))) return rc;
+    if (!p->h_ring_big.empty() && (rc = build_ring_lists(p, bytes))) return rc;
+    return JHTB_OK;
+}
+
+// Azimuthal stage: the range's northern rings and their southern mirrors, split by the
+// kernel that transforms them; within each list the rings keep their order.
+int build_ring_lists(Plan *p, size_t &bytes) {
+    const int T = p->T, t0 = p->ring_t0, t1 = p->ring_t1;
+    int rc;
+    for (int **q : {&p->d_ring_small, &p->d_ring_big})
+        if (*q) cudaFree(*q);
+    p->d_ring_small = p->d_ring_big = nullptr;
+    std::vector<int> small, big;
+    auto add = [&](int r) { (p->h_ring_big[r] ? big : small).push_back(r); };
+    for (int t = t0; t < t1; ++t) {
+        add(t);
+        if (t < T - 1) add(p->nrings - 1 - t);
     }
+    std::sort(small.begin(), small.end());
+    std::sort(big.begin(), big.end());
+    p->nring_small = (int)small.size();
+    p->nring_big = (int)big.size();
+    if ((rc = upload(&p->d_ring_small, small, bytes))) return rc;
+    if ((rc = upload(&p->d_ring_big, big, bytes))) return rc;
     return JHTB_OK;
 }
 
@@ -514,6 +527,22 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
                 d.P = d.N;
                 d.Q = std::max(1, d.N / kFftPiece);
                 d.bh_off = 0;
+            } else if (d.N % 4 == 0 && 2LL * d.N - 1 > kFftPiece && 2LL * (d.N / 4) - 1 <= kFftPiece) {
+                // too long for one shared-memory chirp-z: four of length N / 4 (polar cap rings)
+                const int qn = d.N / 4;
+                d.mode = kSplit4;
+                d.P = (int)next_pow2(2LL * qn - 1);
+                d.Q = 1;
+                auto it = bh_offset.find(qn);
+                if (it == bh_offset.end()) {
+                    bh_offset[qn] = bh_len;
+                    blens.push_back(qn);
+                    boffs.push_back(bh_len);
+                    d.bh_off = bh_len;
+                    bh_len += d.P;
+                } else {
+                    d.bh_off = it->second;
+                }
             } else {
                 d.mode = kBluestein;
                 d.P = (int)next_pow2(2LL * d.N - 1);
@@ -532,6 +561,11 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
             }
         }
         if ((rc = upload(&p->d_rings, rings, bytes))) return rc;
+        p->h_ring_big.assign(nr, 0);
+        for (int r = 0; r < nr; ++r)
+            p->h_ring_big[r] = rings[r].mode == kSplit4 || (rings[r].mode == kDirect && rings[r].N > kFftPiece &&
+                                                           rings[r].N <= kBigN);
+        if ((rc = build_ring_lists(p, bytes))) return rc;
 
         std::vector<double2> tw(kTwLen);
         for (int k = 0; k < kTwLen; ++k) {
@@ -556,7 +590,7 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         bytes += part;
     }
     bool need_w = false;
-    for (auto &d : rings) need_w |= (d.mode == kBluestein || d.Q > 1);
+    for (int r = 0; r < (int)rings.size(); ++r) need_w |= !p->h_ring_big[r] && rings[r].Q > 1;
     if (need_w) {
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_W, sizeof(double2) * (size_t)p->npix * p->chunk));
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_W2, sizeof(double2) * (size_t)p->npix * p->chunk));

@@ -219,27 +219,90 @@ __device__ __forceinline__ double2 bh_get(const double2 *bh, int P, int k, int s
 // with m = k + jN in the first sum and m = jN - k in the second,
 // e^{i m phi0} = (-1)^j e^{+-i pi k / N} when phi0 = pi / N, so
 // D[k] = e^{i pi k / N} [sum_j (-1)^j Fp_{k+jN} + sum_j (-1)^j conj(Fm_{jN-k})];
-// `shifted` selects the (-1)^j signs, the caller applies e^{i pi k / N}.
+// `shifted` selects the (-1)^j signs, the caller applies e^{i pi k / N}.  Aliases
+// j = part, part + parts, ... only (the caller sums the parts in a fixed order).
 __device__ __forceinline__ double2 fold_synth(const double2 *__restrict__ Fp, const double2 *__restrict__ Fm,
-                                              int k, int N, int lmax, bool shifted) {
+                                              int k, int N, int lmax, bool shifted, int part = 0, int parts = 1) {
     double2 d = make_double2(0.0, 0.0);
-    double sg = 1.0;
-    for (int m = k; m <= lmax; m += N) {
+    const double flip = (shifted && (parts & 1)) ? -1.0 : 1.0;  // sign change per step of `parts` aliases
+    double sg = (shifted && (part & 1)) ? -1.0 : 1.0;
+    const int step = parts * N;
+#pragma unroll 4
+    for (int m = k + part * N; m <= lmax; m += step) {
         const double2 f = Fp[m];
         d.x = fma(sg, f.x, d.x);
         d.y = fma(sg, f.y, d.y);
-        if (shifted) sg = -sg;
+        sg *= flip;
     }
-    int m0 = N - k;  // m = jN - k, j >= 1
-    sg = shifted ? -1.0 : 1.0;
-    for (int m = m0; m <= lmax; m += N) {
+    // m = jN - k, j >= 1: alias j = 1 + part, 1 + part + parts, ...
+    sg = (shifted && ((1 + part) & 1)) ? -1.0 : 1.0;
+#pragma unroll 4
+    for (int m = (1 + part) * N - k; m <= lmax; m += step) {
         const double2 f = Fm[m];
         d.x = fma(sg, f.x, d.x);
         d.y = fma(-sg, f.y, d.y);
-        if (shifted) sg = -sg;
+        sg *= flip;
     }
     return d;
 }
+
+// Elements per thread whose global loads are issued together in the azimuthal loops (the
+// loops are bound by L2 / HBM latency, not by arithmetic).
+constexpr int kU = 4;
+
+// The phased (and, for chirp-z, chirped) fold a[k] for k < N into dst[k] (padded shared
+// buffer or a global row).  Rings longer than lmax have at most one term per sum, loaded
+// kU elements at a time; shorter rings split each k's aliases over blockDim / N threads
+// when N < blockDim (partial sums combined in a fixed order through `part_buf`).
+template <bool PADDED>
+__device__ __forceinline__ void synth_fold(const double2 *__restrict__ Fp, const double2 *__restrict__ Fm, int N,
+                                           int lmax, bool shifted, bool blue, double2 *dst, double2 *part_buf) {
+    auto phase = [&](int k, double2 d) {
+        // e^{i pi k / N} ring phase; chirp-z: times w(k) = e^{i pi k^2 / N}
+        const int ph = (shifted ? k : 0) + (blue ? (int)(((long long)k * k) % (2 * N)) : 0);
+        return ph ? cmul(d, cis_pi(ph, N, 0, 1)) : d;
+    };
+    if (N > lmax) {
+        const double sg = shifted ? -1.0 : 1.0;
+        for (int k0 = threadIdx.x; k0 < N; k0 += kU * blockDim.x) {
+            double2 fp[kU], fm[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int k = k0 + u * blockDim.x;
+                fp[u] = (k < N && k <= lmax) ? Fp[k] : make_double2(0.0, 0.0);
+                fm[u] = (k < N && k >= 1 && N - k <= lmax) ? Fm[N - k] : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int k = k0 + u * blockDim.x;
+                if (k < N) {
+                    const double2 d = make_double2(fma(sg, fm[u].x, fp[u].x), fma(-sg, fm[u].y, fp[u].y));
+                    dst[PADDED ? pidx(k) : k] = phase(k, d);
+                }
+            }
+        }
+        return;
+    }
+    const int parts = N < (int)blockDim.x ? (int)blockDim.x / N : 1;
+    if (parts == 1) {
+        for (int k = threadIdx.x; k < N; k += blockDim.x) dst[PADDED ? pidx(k) : k] = phase(k, fold_synth(Fp, Fm, k, N, lmax, shifted));
+        return;
+    }
+    if ((int)threadIdx.x < N * parts) {
+        const int k = threadIdx.x % N, part = threadIdx.x / N;
+        part_buf[threadIdx.x] = fold_synth(Fp, Fm, k, N, lmax, shifted, part, parts);
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < N) {
+        double2 d = part_buf[threadIdx.x];
+        for (int q = 1; q < parts; ++q) d = cadd(d, part_buf[q * N + threadIdx.x]);
+        dst[PADDED ? pidx(threadIdx.x) : threadIdx.x] = phase(threadIdx.x, d);
+    }
+}
+
+// Scratch for the fold's partial sums of short rings (N < blockDim), past the part of the
+// padded FFT buffer such rings use (their transforms have at most 512 points).
+constexpr int kPartOff = 2048;
 
 template <int SPIN>
 __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(const int *__restrict__ ring_list,
@@ -256,20 +319,36 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
     const RingDesc rd = rings[r];
     const int N = rd.N, Q = rd.Q;
     const bool shifted = rd.phi0 != 0.0;
+    const bool blue = rd.mode == kBluestein;
     constexpr int nchan = SPIN ? 2 : 1;
     const double2 *Fp = F_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     const double2 *Fm = SPIN ? Fp + (size_t)nrings * M : Fp;
     double *outQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     double *outU = outQ + npix;
-    if (rd.mode == kDirect && Q == 1) {
-        for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            const double2 d = fold_synth(Fp, Fm, k, N, lmax, shifted);
-            buf[pidx(k)] = shifted ? cmul(d, cis_pi(k, N, 0, 1)) : d;
-        }
+    const int bd = blockDim.x;
+    const double2 *B = bh + rd.bh_off;
+    if (Q == 1) {
+        // the whole transform in shared memory: fold (chirped for chirp-z, zero-padded to P)
+        const int L = blue ? rd.P : N;
+        synth_fold<true>(Fp, Fm, N, lmax, shifted, blue, buf, buf + kPartOff);
+        for (int k = N + threadIdx.x; k < L; k += bd) buf[pidx(k)] = make_double2(0.0, 0.0);
         __syncthreads();
-        fft_stockham(buf, N, +1.0, tw);
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            const double2 v = buf[pidx(j)];
+        if (blue) {
+            fft_stockham(buf, L, -1.0, tw);
+            for (int q0 = threadIdx.x; q0 < L; q0 += kU * bd) {
+                double2 w[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < L ? bh_get(B, L, q0 + u * bd, 1) : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int u = 0; u < kU; ++u)
+                    if (q0 + u * bd < L) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
+            }
+            __syncthreads();
+        }
+        fft_stockham(buf, L, +1.0, tw);
+        for (int j = threadIdx.x; j < N; j += bd) {
+            double2 v = buf[pidx(j)];
+            if (blue) v = cmul(v, cis_pi((int)(((long long)j * j) % (2 * N)), N, 0, 1));
             outQ[j] = v.x;
             if (SPIN) outU[j] = v.y;
         }
@@ -278,32 +357,37 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
     // Transform of length L (N, or the chirp-z length P) in Q pieces of Lp points.  One
     // pass writes the phased (and chirped) fold a[k] to the ring's scratch row; piece s
     // then folds a[k] e^{-+2 pi i s k / L} modulo Lp with table twiddles.
-    const bool blue = rd.mode == kBluestein;
     const int L = blue ? rd.P : N, Lp = L / Q;
     double2 *Ag = A_all + (size_t)blockIdx.y * npix + rd.start;
     double2 *Yg = Y_all + (size_t)blockIdx.y * npix + rd.start;
-    for (int k = threadIdx.x; k < N; k += blockDim.x) {
-        const double2 d = fold_synth(Fp, Fm, k, N, lmax, shifted);
-        // e^{i pi k / N} ring phase; chirp-z: times w(k) = e^{i pi k^2 / N}
-        const int ph = (shifted ? k : 0) + (blue ? (k * k) % (2 * N) : 0);
-        Ag[k] = ph ? cmul(d, cis_pi(ph, N, 0, 1)) : d;
-    }
+    synth_fold<false>(Fp, Fm, N, lmax, shifted, blue, Ag, buf + kPartOff);
     __syncthreads();
-    const double2 *B = bh + rd.bh_off;
     for (int s = 0; s < Q; ++s) {
-        for (int q = threadIdx.x; q < Lp; q += blockDim.x) {
-            double2 v = make_double2(0.0, 0.0);
-            for (int k = q; k < N; k += Lp) {
-                const double2 a = Ag[k];
-                // direct: inverse DFT, e^{+2 pi i s k / N}; chirp-z: FFT_P, e^{-2 pi i s k / P}
-                v = cadd(v, s ? cmul(a, twid(tw, s * k, L, !blue)) : a);
+        for (int q0 = threadIdx.x; q0 < Lp; q0 += kU * bd) {
+            double2 v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) v[u] = make_double2(0.0, 0.0);
+            for (int t = 0; t * Lp < N; ++t) {
+                double2 a[kU], w[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int k = q0 + u * bd + t * Lp;
+                    const bool ok = q0 + u * bd < Lp && k < N;
+                    a[u] = ok ? Ag[k] : make_double2(0.0, 0.0);
+                    // direct: inverse DFT, e^{+2 pi i s k / N}; chirp-z: FFT_P, e^{-2 pi i s k / P}
+                    w[u] = (ok && s) ? twid(tw, s * k, L, !blue) : make_double2(1.0, 0.0);
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) v[u] = cadd(v[u], cmul(a[u], w[u]));
             }
-            buf[pidx(q)] = v;
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (q0 + u * bd < Lp) buf[pidx(q0 + u * bd)] = v[u];
         }
         __syncthreads();
         if (!blue) {
             fft_stockham(buf, Lp, +1.0, tw);
-            for (int q = threadIdx.x; q < Lp; q += blockDim.x) {
+            for (int q = threadIdx.x; q < Lp; q += bd) {
                 const double2 v = buf[pidx(q)];
                 outQ[Q * q + s] = v.x;
                 if (SPIN) outU[Q * q + s] = v.y;
@@ -312,40 +396,71 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
             continue;
         }
         fft_stockham(buf, Lp, -1.0, tw);
-        for (int q = threadIdx.x; q < Lp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, L, Q * q + s, 1));
+        for (int q0 = threadIdx.x; q0 < Lp; q0 += kU * bd) {
+            double2 w[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < Lp ? bh_get(B, L, Q * (q0 + u * bd) + s, 1) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (q0 + u * bd < Lp) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
+        }
         __syncthreads();
         fft_stockham(buf, Lp, +1.0, tw);
         // y[j] += conv_s[j mod Lp] e^{2 pi i s j / P}; the chirp is applied once after the last piece
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            double2 v = buf[pidx(j & (Lp - 1))];
-            if (s) v = cadd(Yg[j], cmul(v, twid(tw, s * j, L, true)));
-            if (s < Q - 1) {
-                Yg[j] = v;
-            } else {
-                v = cmul(v, cis_pi((j * j) % (2 * N), N, 0, 1));
-                outQ[j] = v.x;
-                if (SPIN) outU[j] = v.y;
+        for (int j0 = threadIdx.x; j0 < N; j0 += kU * bd) {
+            double2 y[kU], w[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int j = j0 + u * bd;
+                y[u] = (s && j < N) ? Yg[j] : make_double2(0.0, 0.0);
+                w[u] = (s && j < N) ? twid(tw, s * j, L, true) : make_double2(1.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int j = j0 + u * bd;
+                if (j >= N) continue;
+                double2 v = cadd(y[u], cmul(buf[pidx(j & (Lp - 1))], w[u]));
+                if (s < Q - 1) {
+                    Yg[j] = v;
+                } else {
+                    v = cmul(v, cis_pi((int)(((long long)j * j) % (2 * N)), N, 0, 1));
+                    outQ[j] = v.x;
+                    if (SPIN) outU[j] = v.y;
+                }
             }
         }
         __syncthreads();
     }
 }
 
-// V rows for ring r from its spectrum W (padded shared-memory buffer or natural global).
+// V rows for ring r from its spectrum W (padded shared-memory buffer or natural global),
+// kU orders per thread at a time so the loads of a global W overlap.
 template <int SPIN, bool PADDED>
 __device__ __forceinline__ void gather_adjoint(const double2 *W, int N, int lmax, bool shifted, double2 *Vp,
                                                double2 *Vm) {
-    for (int m = threadIdx.x; m <= lmax; m += blockDim.x) {
-        const int k1 = m % N, k2 = (N - k1) % N;
-        double2 vp = W[PADDED ? pidx(k1) : k1];
-        double2 vm = SPIN ? conjd(W[PADDED ? pidx(k2) : k2]) : vp;
-        if (shifted) {  // e^{-i m phi0} = e^{-i pi m / N}
-            const double2 cph = cis_pi(-(m % (2 * N)), N, 0, 1);
-            vp = cmul(vp, cph);
-            vm = cmul(vm, cph);
+    const int bd = blockDim.x;
+    for (int m0 = threadIdx.x; m0 <= lmax; m0 += kU * bd) {
+        double2 vp[kU], vm[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int m = m0 + u * bd;
+            const int k1 = m % N, k2 = (N - k1) % N;
+            vp[u] = m <= lmax ? W[PADDED ? pidx(k1) : k1] : make_double2(0.0, 0.0);
+            vm[u] = (SPIN && m <= lmax) ? conjd(W[PADDED ? pidx(k2) : k2]) : vp[u];
         }
-        Vp[m] = vp;
-        if (SPIN) Vm[m] = vm;
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int m = m0 + u * bd;
+            if (m > lmax) continue;
+            double2 p = vp[u], q = vm[u];
+            if (shifted) {  // e^{-i m phi0} = e^{-i pi m / N}
+                const double2 cph = cis_pi(-(m % (2 * N)), N, 0, 1);
+                p = cmul(p, cph);
+                q = cmul(q, cph);
+            }
+            Vp[m] = p;
+            if (SPIN) Vm[m] = q;
+        }
     }
 }
 
@@ -364,60 +479,378 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
     const RingDesc rd = rings[r];
     const int N = rd.N, Q = rd.Q;
     const bool shifted = rd.phi0 != 0.0;
+    const bool blue = rd.mode == kBluestein;
     constexpr int nchan = SPIN ? 2 : 1;
     const double *inQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     const double *inU = inQ + npix;
     double2 *Vp = V_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     double2 *Vm = SPIN ? Vp + (size_t)nrings * M : Vp;
-    if (rd.mode == kDirect && Q == 1) {
-        for (int j = threadIdx.x; j < N; j += blockDim.x) buf[pidx(j)] = make_double2(inQ[j], SPIN ? inU[j] : 0.0);
+    const int bd = blockDim.x;
+    const double2 *B = bh + rd.bh_off;
+    // the ring's pixels (chirped for chirp-z: a[j] = v[j] conj(w(j))), kU at a time
+    auto load_in = [&](int j0, double2 (&a)[kU]) {
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int j = j0 + u * bd;
+            a[u] = j < N ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int j = j0 + u * bd;
+            if (blue && j < N) a[u] = cmul(a[u], cis_pi(-(int)(((long long)j * j) % (2 * N)), N, 0, 1));
+        }
+    };
+    if (Q == 1) {
+        // the whole transform in shared memory
+        const int L = blue ? rd.P : N;
+        for (int j0 = threadIdx.x; j0 < N; j0 += kU * bd) {
+            double2 a[kU];
+            load_in(j0, a);
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (j0 + u * bd < N) buf[pidx(j0 + u * bd)] = a[u];
+        }
+        for (int k = N + threadIdx.x; k < L; k += bd) buf[pidx(k)] = make_double2(0.0, 0.0);
         __syncthreads();
-        fft_stockham(buf, N, -1.0, tw);
+        fft_stockham(buf, L, -1.0, tw);
+        if (blue) {
+            for (int q0 = threadIdx.x; q0 < L; q0 += kU * bd) {
+                double2 w[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < L ? bh_get(B, L, q0 + u * bd, -1) : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int u = 0; u < kU; ++u)
+                    if (q0 + u * bd < L) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
+            }
+            __syncthreads();
+            fft_stockham(buf, L, +1.0, tw);
+            // W[k] = conj(w(k)) conv[k]
+            for (int k = threadIdx.x; k < N; k += bd)
+                buf[pidx(k)] = cmul(buf[pidx(k)], cis_pi(-(int)(((long long)k * k) % (2 * N)), N, 0, 1));
+            __syncthreads();
+        }
         gather_adjoint<SPIN, true>(buf, N, lmax, shifted, Vp, Vm);
         return;
     }
     // Forward transform of length L (N, or P) in Q pieces of Lp points; the spectrum
     // W[k], k < N, is assembled in the ring's scratch row and then gathered.
-    const bool blue = rd.mode == kBluestein;
     const int L = blue ? rd.P : N, Lp = L / Q;
     double2 *Ag = A_all + (size_t)blockIdx.y * npix + rd.start;
     double2 *Wg = W_all + (size_t)blockIdx.y * npix + rd.start;
     if (blue) {  // chirped input a[j] = v[j] conj(w(j)), once
-        for (int j = threadIdx.x; j < N; j += blockDim.x)
-            Ag[j] = cmul(make_double2(inQ[j], SPIN ? inU[j] : 0.0), cis_pi(-((j * j) % (2 * N)), N, 0, 1));
+        for (int j0 = threadIdx.x; j0 < N; j0 += kU * bd) {
+            double2 a[kU];
+            load_in(j0, a);
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (j0 + u * bd < N) Ag[j0 + u * bd] = a[u];
+        }
         __syncthreads();
     }
-    const double2 *B = bh + rd.bh_off;
     for (int s = 0; s < Q; ++s) {
-        for (int q = threadIdx.x; q < Lp; q += blockDim.x) {
-            double2 v = make_double2(0.0, 0.0);
-            for (int j = q; j < N; j += Lp) {
-                const double2 a = blue ? Ag[j] : make_double2(inQ[j], SPIN ? inU[j] : 0.0);
-                v = cadd(v, s ? cmul(a, twid(tw, s * j, L, false)) : a);  // e^{-2 pi i s j / L}
+        for (int q0 = threadIdx.x; q0 < Lp; q0 += kU * bd) {
+            double2 v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) v[u] = make_double2(0.0, 0.0);
+            for (int t = 0; t * Lp < N; ++t) {
+                double2 a[kU], w[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int j = q0 + u * bd + t * Lp;
+                    const bool ok = q0 + u * bd < Lp && j < N;
+                    a[u] = !ok ? make_double2(0.0, 0.0) : blue ? Ag[j] : make_double2(inQ[j], SPIN ? inU[j] : 0.0);
+                    w[u] = (ok && s) ? twid(tw, s * j, L, false) : make_double2(1.0, 0.0);  // e^{-2 pi i s j / L}
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) v[u] = cadd(v[u], cmul(a[u], w[u]));
             }
-            buf[pidx(q)] = v;
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (q0 + u * bd < Lp) buf[pidx(q0 + u * bd)] = v[u];
         }
         __syncthreads();
         fft_stockham(buf, Lp, -1.0, tw);
         if (!blue) {  // W[Q q + s]
-            for (int q = threadIdx.x; q < Lp; q += blockDim.x) Wg[Q * q + s] = buf[pidx(q)];
+            for (int q = threadIdx.x; q < Lp; q += bd) Wg[Q * q + s] = buf[pidx(q)];
             __syncthreads();
             continue;
         }
-        for (int q = threadIdx.x; q < Lp; q += blockDim.x) buf[pidx(q)] = cmul(buf[pidx(q)], bh_get(B, L, Q * q + s, -1));
+        for (int q0 = threadIdx.x; q0 < Lp; q0 += kU * bd) {
+            double2 w[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < Lp ? bh_get(B, L, Q * (q0 + u * bd) + s, -1) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (q0 + u * bd < Lp) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
+        }
         __syncthreads();
         fft_stockham(buf, Lp, +1.0, tw);
         // W[k] = conj(w(k)) sum_s conv_s[k mod Lp] e^{2 pi i s k / P}, the chirp after the last piece
-        for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            double2 v = buf[pidx(k & (Lp - 1))];
-            if (s) v = cadd(Wg[k], cmul(v, twid(tw, s * k, L, true)));
-            if (s == Q - 1) v = cmul(v, cis_pi(-((k * k) % (2 * N)), N, 0, 1));
-            Wg[k] = v;
+        for (int k0 = threadIdx.x; k0 < N; k0 += kU * bd) {
+            double2 y[kU], w[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int k = k0 + u * bd;
+                y[u] = (s && k < N) ? Wg[k] : make_double2(0.0, 0.0);
+                w[u] = (s && k < N) ? twid(tw, s * k, L, true) : make_double2(1.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int k = k0 + u * bd;
+                if (k >= N) continue;
+                double2 v = cadd(y[u], cmul(buf[pidx(k & (Lp - 1))], w[u]));
+                if (s == Q - 1) v = cmul(v, cis_pi(-(int)(((long long)k * k) % (2 * N)), N, 0, 1));
+                Wg[k] = v;
+            }
         }
         __syncthreads();
     }
     __threadfence_block();
     gather_adjoint<SPIN, false>(Wg, N, lmax, shifted, Vp, Vm);
+}
+
+// ---------------------------------------------------------------------------------
+// Large rings (N > kFftPiece): 512 threads, one ring per CTA, the whole transform in
+// shared memory (no global scratch).  Direct rings (a power of two N <= kBigN) run one
+// Stockham FFT of N points; kSplit4 rings (N = 4 qn, the long polar-cap rings) run four
+// chirp-z transforms of length qn (power-of-two length P <= kFftPiece) on the decimated
+// sequences and a radix-4 combination:
+//   synthesis  out[j1 + qn j2] = sum_{k2<4} e^{+2 pi i j2 k2 / 4} e^{+2 pi i j1 k2 / N} E_{k2}[j1],
+//              E_{k2}[j1] = sum_{k1<qn} D[4 k1 + k2] e^{+2 pi i j1 k1 / qn}
+//   adjoint    W[k1 + qn k2] = sum_{j2<4} e^{-2 pi i k2 j2 / 4} e^{-2 pi i k1 j2 / N} G_{j2}[k1],
+//              G_{j2}[k1] = sum_{j1<qn} v[4 j1 + j2] e^{-2 pi i k1 j1 / qn}
+// The FFT passes take their twiddles from two small tables in shared memory:
+// e^{-2 pi i x / 8192} = T[x >> 7] T[64 + (x & 127)], T[a] = e^{-2 pi i a / 64},
+// T[64 + b] = e^{-2 pi i b / 8192} (each entry rounded once; the product adds ~1 ulp).
+// ---------------------------------------------------------------------------------
+constexpr int kBigThreads = 512;
+constexpr int kBigBufLen = kBigN + kBigN / 16 + kBigN / 256;  // padded FFT buffer of kBigN points
+constexpr int kBigTwLen = 64 + 128;
+constexpr int kBigBufOff = kBigTwLen;                 // FFT buffer (double2 units)
+constexpr int kBigDOff = kBigTwLen + kFftBufLen;      // kSplit4: the ring's values, natural order
+constexpr int kBigSmemLen = (kBigTwLen + kBigBufLen) > (kBigDOff + kBigN) ? (kBigTwLen + kBigBufLen) : (kBigDOff + kBigN);
+constexpr int kBigSmem = kBigSmemLen * (int)sizeof(double2);
+
+__device__ __forceinline__ double2 big_tw(const double2 *T, int x, bool plus) {  // e^{-+2 pi i x / kBigN}
+    double2 w = cmul(T[x >> 7], T[64 + (x & 127)]);
+    if (plus) w.y = -w.y;
+    return w;
+}
+__device__ __forceinline__ void big_tw_init(double2 *T) {
+    for (int a = threadIdx.x; a < kBigTwLen; a += blockDim.x) {
+        double s, c;
+        if (a < 64) sincospi(-2.0 * (double)a / 64.0, &s, &c);
+        else sincospi(-2.0 * (double)(a - 64) / (double)kBigN, &s, &c);
+        T[a] = make_double2(c, s);
+    }
+}
+
+// One Stockham pass of radix R over n <= kBigN points with kBigThreads threads (the same
+// data movement as stockham_pass).  Twiddles: w = e^{-+2 pi i jm / (Ns R)} from the shared
+// tables, then its powers w^r by complex multiplication (r < R <= 16: at most 15 roundings
+// more than a table entry, far below the transform's own rounding).  Not inlined: each
+// radix gets its own register allocation.
+template <int R, int JM>
+__device__ __noinline__ void big_pass(double2 *buf, int n, int Ns, double dir, const double2 *T) {
+    const int nj = n / R;  // butterflies: at most JM per thread
+    double2 v[JM][R];
+#pragma unroll
+    for (int jj = 0; jj < JM; ++jj) {
+        const int j = threadIdx.x + jj * kBigThreads;
+        if (j < nj) {
+            const int jm = j & (Ns - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[jj][r] = buf[pidx(j + r * nj)];
+            if (Ns > 1) {
+                const double2 w1 = big_tw(T, jm * (kBigN / (Ns * R)), dir > 0);
+                double2 w = w1;
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    v[jj][r] = cmul(v[jj][r], w);
+                    if (r + 1 < R) w = cmul(w, w1);
+                }
+            }
+            reg_fft<R>(v[jj], dir);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < JM; ++jj) {
+        const int j = threadIdx.x + jj * kBigThreads;
+        if (j < nj) {
+            const int jm = j & (Ns - 1);
+            const int d = (j - jm) * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[pidx(d + r * Ns)] = v[jj][r];
+        }
+    }
+    __syncthreads();
+}
+// In-place FFT of length n (power of two, 16 <= n <= kBigN): radix-16 and radix-8 passes
+// only (log2 n = 4 a + 3 b), so every thread holds at most 16 points across a pass.
+__device__ __forceinline__ void fft_big(double2 *buf, int n, double dir, const double2 *T) {
+    static_assert(kBigN == 16 * kBigThreads, "one radix-16 butterfly per thread at kBigN points");
+    int bits = ilog2i(n), Ns = 1;
+    const int n16 = (bits % 3 == 1) ? 1 : (bits % 3 == 2) ? 2 : 0;
+    for (int i = 0; i < n16; ++i, bits -= 4, Ns <<= 4) big_pass<16, 1>(buf, n, Ns, dir, T);
+    if (n > 8 * kBigThreads) {
+        for (; bits >= 3; bits -= 3, Ns <<= 3) big_pass<8, 2>(buf, n, Ns, dir, T);
+    } else {
+        for (; bits >= 3; bits -= 3, Ns <<= 3) big_pass<8, 1>(buf, n, Ns, dir, T);
+    }
+}
+// buf[q] *= Bh(q) for q < P (sgn +1: synthesis spectrum, -1: adjoint), loads kU at a time.
+__device__ __forceinline__ void big_chirp_spectrum(double2 *buf, const double2 *__restrict__ B, int P, int sgn) {
+    for (int q0 = threadIdx.x; q0 < P; q0 += kU * blockDim.x) {
+        double2 w[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) w[u] = q0 + u * (int)blockDim.x < P ? bh_get(B, P, q0 + u * blockDim.x, sgn) : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (q0 + u * (int)blockDim.x < P) buf[pidx(q0 + u * blockDim.x)] = cmul(buf[pidx(q0 + u * blockDim.x)], w[u]);
+    }
+    __syncthreads();
+}
+// One length-qn DFT (sgn +1: e^{+2 pi i jk/qn}, -1: e^{-...}) of the decimated sequence
+// D[4 n + c], n < qn, by chirp-z at length P; the result replaces the sequence in D.
+__device__ __forceinline__ void big_quarter_dft(double2 *D, double2 *buf, int qn, int c, int P, const double2 *__restrict__ B,
+                                                int sgn, const double2 *T) {
+    const int two_q = 2 * qn;
+    for (int n = threadIdx.x; n < P; n += blockDim.x) {
+        double2 a = make_double2(0.0, 0.0);
+        if (n < qn) a = cmul(D[4 * n + c], cis_pi(sgn * (int)(((long long)n * n) % two_q), qn, 0, 1));
+        buf[pidx(n)] = a;
+    }
+    __syncthreads();
+    fft_big(buf, P, -1.0, T);
+    big_chirp_spectrum(buf, B, P, sgn);
+    fft_big(buf, P, +1.0, T);
+    for (int n = threadIdx.x; n < qn; n += blockDim.x)
+        D[4 * n + c] = cmul(buf[pidx(n)], cis_pi(sgn * (int)(((long long)n * n) % two_q), qn, 0, 1));
+    __syncthreads();
+}
+
+template <int SPIN>
+__global__ void __launch_bounds__(kBigThreads, 1) ring_synth_big_kernel(const int *__restrict__ ring_list,
+                                                                        const RingDesc *__restrict__ rings, int lmax,
+                                                                        int M, int nrings, long long npix,
+                                                                        const double2 *__restrict__ F_all,
+                                                                        double *__restrict__ maps_all,
+                                                                        const double2 *__restrict__ bh) {
+    extern __shared__ double2 sm[];
+    double2 *T = sm, *buf = sm + kBigBufOff;
+    const int r = ring_list[blockIdx.x];
+    const RingDesc rd = rings[r];
+    const int N = rd.N;
+    const bool shifted = rd.phi0 != 0.0;
+    constexpr int nchan = SPIN ? 2 : 1;
+    const double2 *Fp = F_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
+    const double2 *Fm = SPIN ? Fp + (size_t)nrings * M : Fp;
+    double *outQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
+    double *outU = outQ + npix;
+    big_tw_init(T);
+    if (rd.mode == kDirect) {
+        synth_fold<true>(Fp, Fm, N, lmax, shifted, false, buf, buf);
+        __syncthreads();
+        fft_big(buf, N, +1.0, T);
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            const double2 v = buf[pidx(j)];
+            outQ[j] = v.x;
+            if (SPIN) outU[j] = v.y;
+        }
+        return;
+    }
+    // kSplit4: phased fold in natural order, four quarter transforms in place, radix-4 combination
+    double2 *D = sm + kBigDOff;
+    const int qn = N / 4;
+    synth_fold<false>(Fp, Fm, N, lmax, shifted, false, D, buf);
+    __syncthreads();
+    for (int c = 0; c < 4; ++c) big_quarter_dft(D, buf, qn, c, rd.P, bh + rd.bh_off, +1, T);
+    for (int j1 = threadIdx.x; j1 < qn; j1 += blockDim.x) {
+        double2 y[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            y[c] = D[4 * j1 + c];
+            if (c) y[c] = cmul(y[c], cis_pi(2 * j1 * c, N, 0, 1));  // e^{+2 pi i j1 c / N}
+        }
+        reg_fft<4>(y, +1.0);
+#pragma unroll
+        for (int j2 = 0; j2 < 4; ++j2) {
+            outQ[j1 + qn * j2] = y[j2].x;
+            if (SPIN) outU[j1 + qn * j2] = y[j2].y;
+        }
+    }
+}
+
+template <int SPIN>
+__global__ void __launch_bounds__(kBigThreads, 1) ring_adjoint_big_kernel(const int *__restrict__ ring_list,
+                                                                          const RingDesc *__restrict__ rings, int lmax,
+                                                                          int M, int nrings, long long npix,
+                                                                          const double *__restrict__ maps_all,
+                                                                          double2 *__restrict__ V_all,
+                                                                          const double2 *__restrict__ bh) {
+    extern __shared__ double2 sm[];
+    double2 *T = sm, *buf = sm + kBigBufOff;
+    const int r = ring_list[blockIdx.x];
+    const RingDesc rd = rings[r];
+    const int N = rd.N;
+    const bool shifted = rd.phi0 != 0.0;
+    constexpr int nchan = SPIN ? 2 : 1;
+    const double *inQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
+    const double *inU = inQ + npix;
+    double2 *Vp = V_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
+    double2 *Vm = SPIN ? Vp + (size_t)nrings * M : Vp;
+    const int bd = blockDim.x;
+    big_tw_init(T);
+    const bool direct = rd.mode == kDirect;
+    double2 *D = direct ? buf : sm + kBigDOff;
+    for (int j0 = threadIdx.x; j0 < N; j0 += kU * bd) {
+        double2 a[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int j = j0 + u * bd;
+            a[u] = j < N ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int j = j0 + u * bd;
+            if (j < N) D[direct ? pidx(j) : j] = a[u];
+        }
+    }
+    __syncthreads();
+    if (direct) {
+        fft_big(buf, N, -1.0, T);
+        gather_adjoint<SPIN, true>(buf, N, lmax, shifted, Vp, Vm);
+        return;
+    }
+    const int qn = N / 4;
+    for (int c = 0; c < 4; ++c) big_quarter_dft(D, buf, qn, c, rd.P, bh + rd.bh_off, -1, T);
+    // radix-4 combination in place: every thread holds its columns' four values first
+    constexpr int KM = (kBigN / 4 + kBigThreads - 1) / kBigThreads;
+    double2 y[KM][4];
+#pragma unroll
+    for (int u = 0; u < KM; ++u) {
+        const int k1 = threadIdx.x + u * kBigThreads;
+        if (k1 < qn) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                y[u][c] = D[4 * k1 + c];
+                if (c) y[u][c] = cmul(y[u][c], cis_pi(-2 * k1 * c, N, 0, 1));  // e^{-2 pi i k1 c / N}
+            }
+            reg_fft<4>(y[u], -1.0);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < KM; ++u) {
+        const int k1 = threadIdx.x + u * kBigThreads;
+        if (k1 < qn) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) D[k1 + qn * c] = y[u][c];
+        }
+    }
+    __syncthreads();
+    gather_adjoint<SPIN, false>(D, N, lmax, shifted, Vp, Vm);
 }
 
 // One block per (Bluestein length, piece): Bh+[Q q + s] = (1/P) sum_n b[n] e^{-2 pi i (Qq+s) n / P}.
@@ -465,40 +898,58 @@ int ensure_smem(K kernel) {
     return JHTB_OK;
 }
 
+template <typename K>
+int ensure_smem_big(K kernel) {
+    JHTB_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBigSmem));
+    return JHTB_OK;
+}
+
+template <int SPIN>
+int launch_ring_synth_t(const Plan &p, const double2 *F, double *maps, int nb, cudaStream_t s) {
+    int rc;
+    if (p.nring_small > 0) {
+        if ((rc = ensure_smem(ring_synth_kernel<SPIN>))) return rc;
+        ring_synth_kernel<SPIN><<<dim3(p.nring_small, nb), kFftThreads, smem_bytes(), s>>>(
+            p.d_ring_small, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F, maps, p.d_W, p.d_W2, p.d_tw, p.d_bh);
+        JHTB_CUDA_TRY(cudaGetLastError());
+    }
+    if (p.nring_big > 0) {
+        if ((rc = ensure_smem_big(ring_synth_big_kernel<SPIN>))) return rc;
+        ring_synth_big_kernel<SPIN><<<dim3(p.nring_big, nb), kBigThreads, kBigSmem, s>>>(
+            p.d_ring_big, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F, maps, p.d_bh);
+        JHTB_CUDA_TRY(cudaGetLastError());
+    }
+    return JHTB_OK;
+}
+
+template <int SPIN>
+int launch_ring_adjoint_t(const Plan &p, const double *maps, double2 *V, double2 *W, int nb, cudaStream_t s) {
+    int rc;
+    if (p.nring_small > 0) {
+        if ((rc = ensure_smem(ring_adjoint_kernel<SPIN>))) return rc;
+        ring_adjoint_kernel<SPIN><<<dim3(p.nring_small, nb), kFftThreads, smem_bytes(), s>>>(
+            p.d_ring_small, p.d_rings, p.lmax, p.M, p.nrings, p.npix, maps, V, p.d_W2, W, p.d_tw, p.d_bh);
+        JHTB_CUDA_TRY(cudaGetLastError());
+    }
+    if (p.nring_big > 0) {
+        if ((rc = ensure_smem_big(ring_adjoint_big_kernel<SPIN>))) return rc;
+        ring_adjoint_big_kernel<SPIN><<<dim3(p.nring_big, nb), kBigThreads, kBigSmem, s>>>(
+            p.d_ring_big, p.d_rings, p.lmax, p.M, p.nrings, p.npix, maps, V, p.d_bh);
+        JHTB_CUDA_TRY(cudaGetLastError());
+    }
+    return JHTB_OK;
+}
+
 }  // namespace
 
 int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;
-    dim3 grid(p.d_ring_list ? p.nring_list : p.nrings, nb);
-    int rc;
-    if (p.spin == 0) {
-        if ((rc = ensure_smem(ring_synth_kernel<0>))) return rc;
-        ring_synth_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
-                                                                     maps, p.d_W, p.d_W2, p.d_tw, p.d_bh);
-    } else {
-        if ((rc = ensure_smem(ring_synth_kernel<2>))) return rc;
-        ring_synth_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F,
-                                                                     maps, p.d_W, p.d_W2, p.d_tw, p.d_bh);
-    }
-    JHTB_CUDA_TRY(cudaGetLastError());
-    return JHTB_OK;
+    return p.spin ? launch_ring_synth_t<2>(p, F, maps, nb, s) : launch_ring_synth_t<0>(p, F, maps, nb, s);
 }
 
 int launch_ring_adjoint(const Plan &p, const double *maps, double2 *V, double2 *W, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;
-    dim3 grid(p.d_ring_list ? p.nring_list : p.nrings, nb);
-    int rc;
-    if (p.spin == 0) {
-        if ((rc = ensure_smem(ring_adjoint_kernel<0>))) return rc;
-        ring_adjoint_kernel<0><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix,
-                                                                       maps, V, p.d_W2, W, p.d_tw, p.d_bh);
-    } else {
-        if ((rc = ensure_smem(ring_adjoint_kernel<2>))) return rc;
-        ring_adjoint_kernel<2><<<grid, kFftThreads, smem_bytes(), s>>>(p.d_ring_list, p.d_rings, p.lmax, p.M, p.nrings, p.npix,
-                                                                       maps, V, p.d_W2, W, p.d_tw, p.d_bh);
-    }
-    JHTB_CUDA_TRY(cudaGetLastError());
-    return JHTB_OK;
+    return p.spin ? launch_ring_adjoint_t<2>(p, maps, V, W, nb, s) : launch_ring_adjoint_t<0>(p, maps, V, W, nb, s);
 }
 
 int launch_bluestein_setup(const Plan &p, const int *lengths, const long long *offs, int nlen, cudaStream_t s) {
