@@ -7,6 +7,7 @@
 // the ring-spectrum workspace.  It replaces jht's lru-cached _prepare
 // (healpix.py:184-357), which builds the same information as NumPy constants.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -619,13 +620,19 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
 
 }  // namespace
 
-// Records an event pair around one stage launch when the plan's timing is on.
+// One stage launch: an NVTX range named after the stage (seen by Nsight Systems /
+// Nsight Compute range filters; a no-op without a tool attached), and, when the
+// plan's timing is on, a CUDA event pair around the launch.
+static const char *const kStageNames[kNumStages] = {"jhtb:legendre_synth", "jhtb:ring_synth", "jhtb:ring_adjoint",
+                                                    "jhtb:legendre_adjoint"};
+
 struct StageTimer {
     Plan &p;
     cudaStream_t s;
     Plan::StageEvent ev{};
     bool on;
     StageTimer(Plan &plan, cudaStream_t stream, int stage) : p(plan), s(stream), on(plan.timing) {
+        nvtxRangePushA(kStageNames[stage]);
         if (!on) return;
         ev.stage = stage;
         if (cudaEventCreate(&ev.start) != cudaSuccess || cudaEventCreate(&ev.stop) != cudaSuccess) {
@@ -635,9 +642,11 @@ struct StageTimer {
         cudaEventRecord(ev.start, s);
     }
     ~StageTimer() {
-        if (!on) return;
-        cudaEventRecord(ev.stop, s);
-        p.events.push_back(ev);
+        if (on) {
+            cudaEventRecord(ev.stop, s);
+            p.events.push_back(ev);
+        }
+        nvtxRangePop();
     }
 };
 
