@@ -62,6 +62,7 @@ def parse_args():
     ap.add_argument("--mixed-batch", type=int, default=16, help="maps per step of the mixed-precision form (0: skip)")
     ap.add_argument("--mixed-steps", type=int, default=3)
     ap.add_argument("--no-configs", action="store_true", help="skip the analysis and 64-map batch lines")
+    ap.add_argument("--cg-iters", type=int, default=100, help="CG iterations timed per precision in the CG line (0: skip)")
     ap.add_argument("--offgrid-points", type=int, default=10_000_000,
                     help="points of the secondary off-grid measurement (0: skip)")
     return ap.parse_args()
@@ -367,6 +368,68 @@ def run_configs(jhtb, _lib, torch, dev) -> dict:
     return out
 
 
+def cg_problem(jhtb, torch, nside: int = 512, lmax: int = 1024, B: int = 16, seed: int = 16):
+    """The masked CG deconvolution workload: spin 0, a |cos theta| < 0.34 cut plus 200 seeded
+    1-degree discs, data S a + white noise (sigma 1e-2) for B right-hand sides, and
+    eps = 1e-6 of the largest diagonal entry of T S^T (M W) S T^-1 (probed on 16 m = 0 columns)."""
+    from jht_b200 import masked as MK
+
+    npix = 12 * nside * nside
+    rng = np.random.default_rng(seed)
+    geo = jhtb.healpix.RingInfo(nside)
+    z = np.repeat(geo.z, geo.npix_ring)
+    phi = np.concatenate([geo.phi0[r] + 2 * np.pi * np.arange(n) / n for r, n in enumerate(geo.npix_ring)])
+    st = np.sqrt(1 - z * z)
+    mask = (np.abs(z) >= 0.34).astype(np.float64)
+    cz = rng.uniform(-1, 1, 200)
+    cp = rng.uniform(0, 2 * np.pi, 200)
+    cs = np.sqrt(1 - cz * cz)
+    cos_r = np.cos(np.radians(1.0))
+    for k in range(200):
+        mask[z * cz[k] + st * cs[k] * np.cos(phi - cp[k]) > cos_r] = 0.0
+    ell = np.concatenate([np.arange(m, lmax + 1) for m in range(lmax + 1)])
+    K = jhtb.alm_size(lmax)
+    cl = 1.0 / (ell + 10.0) ** 2
+    a = np.sqrt(cl / 2) * (rng.standard_normal((B, K)) + 1j * rng.standard_normal((B, K)))
+    a[:, : lmax + 1] = np.sqrt(cl[: lmax + 1]) * rng.standard_normal((B, lmax + 1))
+    gen = torch.Generator("cuda").manual_seed(seed)
+    maps = jhtb.synthesis_batch(a, nside, lmax, 0)
+    maps = maps + 1e-2 * torch.randn(maps.shape, dtype=torch.float64, device="cuda", generator=gen)
+    w = MK._weight_pix(nside, npix, maps.device, mask=mask)
+    probe = torch.zeros((16, MK.n_dof(lmax, 0)), dtype=torch.float64, device="cuda")
+    cols = torch.as_tensor(np.linspace(0, lmax, 16).astype(np.int64), device="cuda")
+    probe[torch.arange(16, device="cuda"), cols] = 1.0
+    diag = MK._normal(probe, w, nside, lmax, 0, "fp64")[torch.arange(16, device="cuda"), cols]
+    return maps, mask, 1e-6 * float(diag.max())
+
+
+def run_cg(jhtb, torch, iters: int) -> dict:
+    """Secondary line: the 16-RHS masked CG at nside 512 / lmax 1024, a bounded number of
+    iterations per precision (the solve to relative residual 1e-8 takes thousands of
+    iterations at eps = 1e-6 and runs in the GPU test suite); ms per iteration, the
+    residual reached, and the per-iteration operator work S + S^T on 16 maps."""
+    nside, lmax, B = 512, 1024, 16
+    maps, mask, eps = cg_problem(jhtb, torch, nside, lmax, B)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    out = {"workload": f"masked CG (|cos theta| < 0.34 cut + 200 discs of 1 deg), spin 0, nside {nside}, "
+                       f"lmax {lmax}, {B} right-hand sides, eps = 1e-6 of the largest diagonal; "
+                       f"{iters} iterations timed per precision", "eps": eps}
+    for prec in ("fp64", "bf16x3"):
+        jhtb.deconvolve_batch(maps, mask, nside, lmax, 0, tol=1e-8, reg=eps, max_iter=2, precision=prec)
+        torch.cuda.synchronize()
+        ev[0].record()
+        _, info = jhtb.deconvolve_batch(maps, mask, nside, lmax, 0, tol=1e-8, reg=eps, max_iter=iters,
+                                        return_info=True, precision=prec)
+        ev[1].record()
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        out[prec] = {"ms": ms, "iterations": info["iterations"], "ms_per_iteration": ms / max(info["iterations"], 1),
+                     "rel_residual_max": float(info["rel_residual"].max()),
+                     "fp64_residual_replacements": info.get("outer", 0)}
+    out["mixed_vs_fp64_per_iteration"] = out["fp64"]["ms_per_iteration"] / out["bf16x3"]["ms_per_iteration"]
+    return out
+
+
 def run_offgrid(jhtb, torch, dev, npts: int, lmax: int = 2048, spin: int = 2, reps: int = 3) -> dict:
     """Secondary line: off-grid synthesis_general and its adjoint (spin 2, lmax 2048) at
     seeded uniform points, device-resident, CUDA-event timed."""
@@ -603,6 +666,8 @@ def main():
 
     offgrid = run_offgrid(jhtb, torch, dev, args.offgrid_points) if args.offgrid_points > 0 else None
     configs = run_configs(jhtb, _lib, torch, dev) if not args.no_configs else None
+    if configs is not None and args.cg_iters > 0:
+        configs["cg16_n512_l1024"] = run_cg(jhtb, torch, args.cg_iters)
 
     cpu = None
     if not args.no_cpu_baseline:

@@ -68,7 +68,6 @@ constexpr int kFftLogMax = 13;
 // Ring FFT modes: kDirect (N a power of two), kBluestein (chirp-z of length N), kSplit4
 // (N = 4 i: four chirp-z transforms of length i and a radix-4 combination).
 enum RingMode : int { kDirect = 0, kBluestein = 1, kSplit4 = 2 };
-constexpr int kBigN = 8192;      // largest ring transform held whole in shared memory (large-ring kernel)
 
 struct RingDesc {
     int N;          // pixels in the ring
@@ -80,6 +79,14 @@ struct RingDesc {
     long long bh_off;  // offset (complex units) of this length's chirp spectrum
     double phi0;       // azimuth of the first pixel
 };
+
+// Pieces a ring's transform runs in, one CTA each (1: the whole ring in one CTA): a
+// power-of-two ring above kFftPiece points in N / kFftPiece pieces, a kSplit4 ring in 4.
+__host__ __device__ __forceinline__ int ring_pieces(const RingDesc &rd) {
+    if (rd.mode == kSplit4) return 4;
+    if (rd.mode == kDirect && rd.N > kFftPiece && 2 * rd.N <= kTwLen) return rd.N / kFftPiece;
+    return 1;
+}
 
 // Per-m seed parameters.  Spin 0: lf = theta-independent log|lambda_mm|,
 // sign = (-1)^m, pc = ps = 0.  Spin +-2: log|d^{lmin}_{-m,+-2}| = lf + pc log cos(t/2)
@@ -194,11 +201,11 @@ struct Plan {
     int nsynth;           // entries of d_synth_order (items inside the range)
     int tc_norder;        // entries of d_tc_order
     // rings of the plan's range by kernel: ring_small (one 256-thread CTA per ring, pieces
-    // through global scratch above kFftPiece points) and ring_big (512 threads, the whole
-    // transform of up to kBigN points in shared memory)
-    int *d_ring_small, *d_ring_big;
-    int nring_small, nring_big;
-    std::vector<unsigned char> h_ring_big;  // [ring] 1 when the large-ring kernel takes it
+    // through global scratch above kFftPiece points) and ring_piece ((ring << 3 | piece)
+    // work units of the rings that run in pieces, ring_pieces() > 1)
+    int *d_ring_small, *d_ring_piece;
+    int nring_small, nring_piece;
+    std::vector<unsigned char> h_ring_pieces;  // [ring] pieces of its transform (1: the one-CTA kernel)
     std::vector<int> h_lw, h_a_lw, h_tc_lw;  // start l per item, kept for re-sorting
 
     // workspace

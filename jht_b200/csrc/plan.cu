@@ -90,7 +90,7 @@ void free_plan(Plan *p) {
     void *ptrs[] = {p->d_x,     p->d_logsin, p->d_logch, p->d_logsh,   p->d_rings, p->d_tw,
                     p->d_bh,    p->d_seed,   p->d_alpha, p->d_gamma,   p->d_cnorm, p->d_F,
                     p->d_W,     p->d_W2,     p->d_scratch, p->d_lw, p->d_st, p->d_stsc, p->d_synth_order,
-                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err, p->d_ring_small, p->d_ring_big};
+                    p->d_adj_order, p->d_adj_tiles, p->d_counter, p->d_part, p->d_err, p->d_ring_small, p->d_ring_piece};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (p->a_owns_tables) {
@@ -220,30 +220,35 @@ int build_orders(Plan *p) {
         p->d_tca_items = nullptr;
         if ((rc = upload(&p->d_tca_items, items, bytes))) return rc;
     }
-    if (!p->h_ring_big.empty() && (rc = build_ring_lists(p, bytes))) return rc;
+    if (!p->h_ring_pieces.empty() && (rc = build_ring_lists(p, bytes))) return rc;
     return JHTB_OK;
 }
 
 // Azimuthal stage: the range's northern rings and their southern mirrors, split by the
-// kernel that transforms them; within each list the rings keep their order.
+// kernel that transforms them (whole rings in one CTA; (ring << 3 | piece) units of the
+// rings that run in pieces, a ring's pieces adjacent so that they read its data from L2
+// together); within each list the rings keep their order.
 int build_ring_lists(Plan *p, size_t &bytes) {
     const int T = p->T, t0 = p->ring_t0, t1 = p->ring_t1;
     int rc;
-    for (int **q : {&p->d_ring_small, &p->d_ring_big})
+    for (int **q : {&p->d_ring_small, &p->d_ring_piece})
         if (*q) cudaFree(*q);
-    p->d_ring_small = p->d_ring_big = nullptr;
-    std::vector<int> small, big;
-    auto add = [&](int r) { (p->h_ring_big[r] ? big : small).push_back(r); };
+    p->d_ring_small = p->d_ring_piece = nullptr;
+    std::vector<int> small, whole;
+    auto add = [&](int r) { (p->h_ring_pieces[r] > 1 ? whole : small).push_back(r); };
     for (int t = t0; t < t1; ++t) {
         add(t);
         if (t < T - 1) add(p->nrings - 1 - t);
     }
     std::sort(small.begin(), small.end());
-    std::sort(big.begin(), big.end());
+    std::sort(whole.begin(), whole.end());
+    std::vector<int> pieces;
+    for (int r : whole)
+        for (int s = 0; s < p->h_ring_pieces[r]; ++s) pieces.push_back(r << 3 | s);
     p->nring_small = (int)small.size();
-    p->nring_big = (int)big.size();
+    p->nring_piece = (int)pieces.size();
     if ((rc = upload(&p->d_ring_small, small, bytes))) return rc;
-    if ((rc = upload(&p->d_ring_big, big, bytes))) return rc;
+    if ((rc = upload(&p->d_ring_piece, pieces, bytes))) return rc;
     return JHTB_OK;
 }
 
@@ -562,10 +567,8 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
             }
         }
         if ((rc = upload(&p->d_rings, rings, bytes))) return rc;
-        p->h_ring_big.assign(nr, 0);
-        for (int r = 0; r < nr; ++r)
-            p->h_ring_big[r] = rings[r].mode == kSplit4 || (rings[r].mode == kDirect && rings[r].N > kFftPiece &&
-                                                           rings[r].N <= kBigN);
+        p->h_ring_pieces.assign(nr, 1);
+        for (int r = 0; r < nr; ++r) p->h_ring_pieces[r] = (unsigned char)ring_pieces(rings[r]);
         if ((rc = build_ring_lists(p, bytes))) return rc;
 
         std::vector<double2> tw(kTwLen);
@@ -591,7 +594,7 @@ int build_plan(Plan *p, const jhtb_host_tables *ht) {
         bytes += part;
     }
     bool need_w = false;
-    for (int r = 0; r < (int)rings.size(); ++r) need_w |= !p->h_ring_big[r] && rings[r].Q > 1;
+    for (int r = 0; r < (int)rings.size(); ++r) need_w |= p->h_ring_pieces[r] == 1 && rings[r].Q > 1;
     if (need_w) {
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_W, sizeof(double2) * (size_t)p->npix * p->chunk));
         JHTB_CUDA_TRY(cudaMalloc((void **)&p->d_W2, sizeof(double2) * (size_t)p->npix * p->chunk));

@@ -207,6 +207,71 @@ __device__ __forceinline__ void fft_stockham(double2 *buf, int n, double dir, co
     else if (bits == 1) stockham_pass_call<2>(buf, n, Ns, dir, tw);
 }
 
+// Twiddles from shared memory: e^{-2 pi i x / kFftPiece} = T[x >> 6] T[64 + (x & 63)] with
+// T[a] = e^{-2 pi i a / 64} and T[64 + b] = e^{-2 pi i b / kFftPiece} (each entry rounded once,
+// the product adds about one rounding), so the passes make no global loads.
+constexpr int kSmTwLen = 128;
+static_assert(kFftPiece == 64 * 64, "two-level twiddle table of kFftPiece points");
+__device__ __forceinline__ void sm_tw_init(double2 *T) {
+    for (int a = threadIdx.x; a < kSmTwLen; a += blockDim.x) {
+        double s, c;
+        if (a < 64) sincospi(-2.0 * (double)a / 64.0, &s, &c);
+        else sincospi(-2.0 * (double)(a - 64) / (double)kFftPiece, &s, &c);
+        T[a] = make_double2(c, s);
+    }
+}
+__device__ __forceinline__ double2 sm_tw(const double2 *T, int x, bool plus) {  // e^{-+2 pi i x / kFftPiece}
+    x &= kFftPiece - 1;
+    double2 w = cmul(T[x >> 6], T[64 + (x & 63)]);
+    if (plus) w.y = -w.y;
+    return w;
+}
+
+// stockham_pass with the shared-memory twiddle table.
+template <int R>
+__device__ __forceinline__ void stockham_pass_sm(double2 *buf, int n, int Ns, double dir, const double2 *T) {
+    constexpr int JM = kFftPiece / (R * kFftThreads);
+    const int nj = n / R;
+    double2 v[JM][R];
+#pragma unroll
+    for (int jj = 0; jj < JM; ++jj) {
+        const int j = threadIdx.x + jj * kFftThreads;
+        if (j < nj) {
+            const int jm = j & (Ns - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[jj][r] = buf[pidx(j + r * nj)];
+            if (Ns > 1) {
+                const int step = jm * (kFftPiece / (Ns * R));
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[jj][r] = cmul(v[jj][r], sm_tw(T, step * r, dir > 0));
+            }
+            reg_fft<R>(v[jj], dir);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < JM; ++jj) {
+        const int j = threadIdx.x + jj * kFftThreads;
+        if (j < nj) {
+            const int jm = j & (Ns - 1);
+            const int d = (j - jm) * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[pidx(d + r * Ns)] = v[jj][r];
+        }
+    }
+    __syncthreads();
+}
+
+// The FFT with every pass inlined (no call boundary, so no register saves to the stack
+// around the passes) and shared-memory twiddles; for kernels that run one or two transforms.
+__device__ __forceinline__ void fft_stockham_sm(double2 *buf, int n, double dir, const double2 *T) {
+    int bits = ilog2i(n), Ns = 1;
+    for (; bits >= 4; bits -= 4, Ns <<= 4) stockham_pass_sm<16>(buf, n, Ns, dir, T);
+    if (bits == 3) stockham_pass_sm<8>(buf, n, Ns, dir, T);
+    else if (bits == 2) stockham_pass_sm<4>(buf, n, Ns, dir, T);
+    else if (bits == 1) stockham_pass_sm<2>(buf, n, Ns, dir, T);
+}
+
 // Bluestein spectrum for the synthesis direction: Bh+ = FFT_P(b)/P with
 // b[n] = conj(w(n)) on |n| < N, w(n) = e^{+i pi n^2 / N}.  The adjoint direction
 // uses Bh-[k] = conj(Bh+[(P - k) mod P]).
@@ -610,190 +675,157 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
 }
 
 // ---------------------------------------------------------------------------------
-// Large rings (N > kFftPiece): 512 threads, one ring per CTA, the whole transform in
-// shared memory (no global scratch).  Direct rings (a power of two N <= kBigN) run one
-// Stockham FFT of N points; kSplit4 rings (N = 4 qn, the long polar-cap rings) run four
-// chirp-z transforms of length qn (power-of-two length P <= kFftPiece) on the decimated
-// sequences and a radix-4 combination:
-//   synthesis  out[j1 + qn j2] = sum_{k2<4} e^{+2 pi i j2 k2 / 4} e^{+2 pi i j1 k2 / N} E_{k2}[j1],
-//              E_{k2}[j1] = sum_{k1<qn} D[4 k1 + k2] e^{+2 pi i j1 k1 / qn}
-//   adjoint    W[k1 + qn k2] = sum_{j2<4} e^{-2 pi i k2 j2 / 4} e^{-2 pi i k1 j2 / N} G_{j2}[k1],
-//              G_{j2}[k1] = sum_{j1<qn} v[4 j1 + j2] e^{-2 pi i k1 j1 / qn}
-// The FFT passes take their twiddles from two small tables in shared memory:
-// e^{-2 pi i x / 8192} = T[x >> 7] T[64 + (x & 127)], T[a] = e^{-2 pi i a / 64},
-// T[64 + b] = e^{-2 pi i b / 8192} (each entry rounded once; the product adds ~1 ulp).
+// Long rings in pieces: a ring of N = Q Lq points (a power of two above kFftPiece, Lq =
+// kFftPiece; or a kSplit4 polar-cap ring, N = 4 Lq with Lq not a power of two) runs as Q
+// independent CTAs of the 256-thread shared-memory kernel, one per output residue class
+// (decimation in frequency).  Piece s:
+//   synthesis  out[Q j + s] = sum_{k1 < Lq} e^{+2 pi i j k1 / Lq} a_s[k1],
+//              a_s[k1]      = sum_{k2 < Q} D[k1 + Lq k2] e^{+2 pi i s (k1 + Lq k2) / N}
+//   adjoint    W[Q k + s]   = sum_{j1 < Lq} e^{-2 pi i k j1 / Lq} b_s[j1],
+//              b_s[j1]      = sum_{j2 < Q} v[j1 + Lq j2] e^{-2 pi i s (j1 + Lq j2) / N}
+// with D the phased fold of the synthesis and v the ring's pixels.  The length-Lq
+// transform is the Stockham FFT (power of two) or a chirp-z transform at P <= kFftPiece
+// points (kSplit4).  Every piece gathers the whole ring's input itself (the Q reads of a
+// ring's data hit L2), so pieces never exchange data and several fit on an SM at once.
 // ---------------------------------------------------------------------------------
-constexpr int kBigThreads = 512;
-constexpr int kBigBufLen = kBigN + kBigN / 16 + kBigN / 256;  // padded FFT buffer of kBigN points
-constexpr int kBigTwLen = 64 + 128;
-constexpr int kBigBufOff = kBigTwLen;                 // FFT buffer (double2 units)
-constexpr int kBigDOff = kBigTwLen + kFftBufLen;      // kSplit4: the ring's values, natural order
-constexpr int kBigSmemLen = (kBigTwLen + kBigBufLen) > (kBigDOff + kBigN) ? (kBigTwLen + kBigBufLen) : (kBigDOff + kBigN);
-constexpr int kBigSmem = kBigSmemLen * (int)sizeof(double2);
-
-__device__ __forceinline__ double2 big_tw(const double2 *T, int x, bool plus) {  // e^{-+2 pi i x / kBigN}
-    double2 w = cmul(T[x >> 7], T[64 + (x & 127)]);
-    if (plus) w.y = -w.y;
+// e^{+i pi a / N} for a power-of-two N <= kTwLen / 2, from the twiddle table (entries
+// e^{-2 pi i j / kTwLen}, each rounded once).
+__device__ __forceinline__ double2 tw_pi(const double2 *__restrict__ tw, long long a, int N) {
+    const int r = (int)(a & (2LL * N - 1));
+    double2 w = __ldg(&tw[r * (kTwLen / (2 * N))]);
+    w.y = -w.y;
     return w;
 }
-__device__ __forceinline__ void big_tw_init(double2 *T) {
-    for (int a = threadIdx.x; a < kBigTwLen; a += blockDim.x) {
-        double s, c;
-        if (a < 64) sincospi(-2.0 * (double)a / 64.0, &s, &c);
-        else sincospi(-2.0 * (double)(a - 64) / (double)kBigN, &s, &c);
-        T[a] = make_double2(c, s);
+// most pieces of a ring (ring_pieces: a power of two N <= kTwLen / 2 in N / kFftPiece, kSplit4 in 4)
+constexpr int kMaxPieces = 4;
+static_assert(kTwLen / 2 / kFftPiece <= kMaxPieces, "pieces of the longest power-of-two ring");
+
+// e^{i pi k / 4}, k mod 8
+__device__ __forceinline__ double2 root8(int k) {
+    constexpr double h = 0.70710678118654752440;
+    switch (k & 7) {
+        case 0: return make_double2(1.0, 0.0);
+        case 1: return make_double2(h, h);
+        case 2: return make_double2(0.0, 1.0);
+        case 3: return make_double2(-h, h);
+        case 4: return make_double2(-1.0, 0.0);
+        case 5: return make_double2(-h, -h);
+        case 6: return make_double2(0.0, -1.0);
+        default: return make_double2(h, -h);
     }
 }
 
-// One Stockham pass of radix R over n <= kBigN points with kBigThreads threads (the same
-// data movement as stockham_pass).  Twiddles: w = e^{-+2 pi i jm / (Ns R)} from the shared
-// tables, then its powers w^r by complex multiplication (r < R <= 16: at most 15 roundings
-// more than a table entry, far below the transform's own rounding).  Not inlined: each
-// radix gets its own register allocation.
-template <int R, int JM>
-__device__ __noinline__ void big_pass(double2 *buf, int n, int Ns, double dir, const double2 *T) {
-    const int nj = n / R;  // butterflies: at most JM per thread
-    double2 v[JM][R];
-#pragma unroll
-    for (int jj = 0; jj < JM; ++jj) {
-        const int j = threadIdx.x + jj * kBigThreads;
-        if (j < nj) {
-            const int jm = j & (Ns - 1);
-#pragma unroll
-            for (int r = 0; r < R; ++r) v[jj][r] = buf[pidx(j + r * nj)];
-            if (Ns > 1) {
-                const double2 w1 = big_tw(T, jm * (kBigN / (Ns * R)), dir > 0);
-                double2 w = w1;
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    v[jj][r] = cmul(v[jj][r], w);
-                    if (r + 1 < R) w = cmul(w, w1);
-                }
-            }
-            reg_fft<R>(v[jj], dir);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int jj = 0; jj < JM; ++jj) {
-        const int j = threadIdx.x + jj * kBigThreads;
-        if (j < nj) {
-            const int jm = j & (Ns - 1);
-            const int d = (j - jm) * R + jm;
-#pragma unroll
-            for (int r = 0; r < R; ++r) buf[pidx(d + r * Ns)] = v[jj][r];
-        }
-    }
-    __syncthreads();
-}
-// In-place FFT of length n (power of two, 16 <= n <= kBigN): radix-16 and radix-8 passes
-// only (log2 n = 4 a + 3 b), so every thread holds at most 16 points across a pass.
-__device__ __forceinline__ void fft_big(double2 *buf, int n, double dir, const double2 *T) {
-    static_assert(kBigN == 16 * kBigThreads, "one radix-16 butterfly per thread at kBigN points");
-    int bits = ilog2i(n), Ns = 1;
-    const int n16 = (bits % 3 == 1) ? 1 : (bits % 3 == 2) ? 2 : 0;
-    for (int i = 0; i < n16; ++i, bits -= 4, Ns <<= 4) big_pass<16, 1>(buf, n, Ns, dir, T);
-    if (n > 8 * kBigThreads) {
-        for (; bits >= 3; bits -= 3, Ns <<= 3) big_pass<8, 2>(buf, n, Ns, dir, T);
-    } else {
-        for (; bits >= 3; bits -= 3, Ns <<= 3) big_pass<8, 1>(buf, n, Ns, dir, T);
-    }
-}
-// buf[q] *= Bh(q) for q < P (sgn +1: synthesis spectrum, -1: adjoint), loads kU at a time.
-__device__ __forceinline__ void big_chirp_spectrum(double2 *buf, const double2 *__restrict__ B, int P, int sgn) {
-    for (int q0 = threadIdx.x; q0 < P; q0 += kU * blockDim.x) {
-        double2 w[kU];
-#pragma unroll
-        for (int u = 0; u < kU; ++u) w[u] = q0 + u * (int)blockDim.x < P ? bh_get(B, P, q0 + u * blockDim.x, sgn) : make_double2(0.0, 0.0);
-#pragma unroll
-        for (int u = 0; u < kU; ++u)
-            if (q0 + u * (int)blockDim.x < P) buf[pidx(q0 + u * blockDim.x)] = cmul(buf[pidx(q0 + u * blockDim.x)], w[u]);
-    }
-    __syncthreads();
-}
-// One length-qn DFT (sgn +1: e^{+2 pi i jk/qn}, -1: e^{-...}) of the decimated sequence
-// D[4 n + c], n < qn, by chirp-z at length P; the result replaces the sequence in D.
-__device__ __forceinline__ void big_quarter_dft(double2 *D, double2 *buf, int qn, int c, int P, const double2 *__restrict__ B,
-                                                int sgn, const double2 *T) {
-    const int two_q = 2 * qn;
-    for (int n = threadIdx.x; n < P; n += blockDim.x) {
-        double2 a = make_double2(0.0, 0.0);
-        if (n < qn) a = cmul(D[4 * n + c], cis_pi(sgn * (int)(((long long)n * n) % two_q), qn, 0, 1));
-        buf[pidx(n)] = a;
-    }
-    __syncthreads();
-    fft_big(buf, P, -1.0, T);
-    big_chirp_spectrum(buf, B, P, sgn);
-    fft_big(buf, P, +1.0, T);
-    for (int n = threadIdx.x; n < qn; n += blockDim.x)
-        D[4 * n + c] = cmul(buf[pidx(n)], cis_pi(sgn * (int)(((long long)n * n) % two_q), qn, 0, 1));
-    __syncthreads();
+// D[k] of the synthesis fold without its ring phase (see fold_synth); one term per sum
+// when the ring is longer than lmax.
+__device__ __forceinline__ double2 fold_one(const double2 *__restrict__ Fp, const double2 *__restrict__ Fm, int k, int N,
+                                            int lmax, bool shifted) {
+    if (N <= lmax) return fold_synth(Fp, Fm, k, N, lmax, shifted);
+    const double2 fp = k <= lmax ? Fp[k] : make_double2(0.0, 0.0);
+    const double2 fm = (k >= 1 && N - k <= lmax) ? Fm[N - k] : make_double2(0.0, 0.0);
+    const double sg = shifted ? -1.0 : 1.0;
+    return make_double2(fma(sg, fm.x, fp.x), fma(-sg, fm.y, fp.y));
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kBigThreads, 1) ring_synth_big_kernel(const int *__restrict__ ring_list,
-                                                                        const RingDesc *__restrict__ rings, int lmax,
-                                                                        int M, int nrings, long long npix,
-                                                                        const double2 *__restrict__ F_all,
-                                                                        double *__restrict__ maps_all,
-                                                                        const double2 *__restrict__ bh) {
-    extern __shared__ double2 sm[];
-    double2 *T = sm, *buf = sm + kBigBufOff;
-    const int r = ring_list[blockIdx.x];
+__global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_piece_kernel(const int *__restrict__ piece_list,
+                                                                           const RingDesc *__restrict__ rings, int lmax,
+                                                                           int M, int nrings, long long npix,
+                                                                           const double2 *__restrict__ F_all,
+                                                                           double *__restrict__ maps_all,
+                                                                           const double2 *__restrict__ tw,
+                                                                           const double2 *__restrict__ bh) {
+    extern __shared__ double2 buf[];
+    double2 *T = buf + kFftBufLen;  // twiddle table after the FFT buffer
+    sm_tw_init(T);
+    const int code = piece_list[blockIdx.x];
+    const int r = code >> 3, s = code & 7;
     const RingDesc rd = rings[r];
-    const int N = rd.N;
+    const int N = rd.N, Q = ring_pieces(rd), Lq = N / Q;
+    const bool split = rd.mode == kSplit4;
     const bool shifted = rd.phi0 != 0.0;
+    const int c = (shifted ? 1 : 0) + 2 * s;  // term k carries e^{i pi c k / N} (ring phase and piece twiddle)
     constexpr int nchan = SPIN ? 2 : 1;
     const double2 *Fp = F_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     const double2 *Fm = SPIN ? Fp + (size_t)nrings * M : Fp;
     double *outQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     double *outU = outQ + npix;
-    big_tw_init(T);
-    if (rd.mode == kDirect) {
-        synth_fold<true>(Fp, Fm, N, lmax, shifted, false, buf, buf);
-        __syncthreads();
-        fft_big(buf, N, +1.0, T);
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            const double2 v = buf[pidx(j)];
-            outQ[j] = v.x;
-            if (SPIN) outU[j] = v.y;
+    const int bd = blockDim.x;
+    // a_s[k1]: the Q aliases k1 + Lq k2 of the phased fold, kU values of k1 per thread at a time
+    for (int k10 = threadIdx.x; k10 < Lq; k10 += kU * bd) {
+        double2 acc[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) acc[u] = make_double2(0.0, 0.0);
+        // every load of the kU x Q terms is issued before the first is used
+        double2 d[kMaxPieces][kU];
+#pragma unroll
+        for (int k2 = 0; k2 < kMaxPieces; ++k2)
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int k1 = k10 + u * bd;
+                d[k2][u] = (k2 < Q && k1 < Lq) ? fold_one(Fp, Fm, k1 + Lq * k2, N, lmax, shifted) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+        for (int k2 = 0; k2 < kMaxPieces; ++k2) {
+            if (k2 >= Q) break;
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int k1 = k10 + u * bd;
+                // power of two: e^{i pi c k / N} exactly from the table; kSplit4: the k2 part of
+                // e^{i pi c (k1 + Lq k2) / N} = e^{i pi c k1 / N} e^{i pi c k2 / 4} (the k1 part below)
+                const double2 w = split ? root8(c * k2) : tw_pi(tw, (long long)c * (k1 + Lq * k2), N);
+                acc[u] = cadd(acc[u], cmul(d[k2][u], w));
+            }
         }
-        return;
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int k1 = k10 + u * bd;
+            if (k1 >= Lq) continue;
+            double2 v = acc[u];
+            // kSplit4: e^{i pi c k1 / N} times the chirp w(k1) = e^{i pi k1^2 / Lq} = e^{i pi 4 k1^2 / N}
+            if (split) v = cmul(v, cis_pi((int)(((long long)c * k1 + 4LL * k1 * k1) % (2LL * N)), N, 0, 1));
+            buf[pidx(k1)] = v;
+        }
     }
-    // kSplit4: phased fold in natural order, four quarter transforms in place, radix-4 combination
-    double2 *D = sm + kBigDOff;
-    const int qn = N / 4;
-    synth_fold<false>(Fp, Fm, N, lmax, shifted, false, D, buf);
+    const int L = split ? rd.P : Lq;
+    for (int k = Lq + threadIdx.x; k < L; k += bd) buf[pidx(k)] = make_double2(0.0, 0.0);
     __syncthreads();
-    for (int c = 0; c < 4; ++c) big_quarter_dft(D, buf, qn, c, rd.P, bh + rd.bh_off, +1, T);
-    for (int j1 = threadIdx.x; j1 < qn; j1 += blockDim.x) {
-        double2 y[4];
+    if (split) {  // E[j] = w(j) sum_k (a[k] w(k)) conj(w(j - k)): FFT, chirp spectrum, inverse FFT
+        fft_stockham_sm(buf, L, -1.0, T);
+        for (int q0 = threadIdx.x; q0 < L; q0 += kU * bd) {
+            double2 w[kU];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            y[c] = D[4 * j1 + c];
-            if (c) y[c] = cmul(y[c], cis_pi(2 * j1 * c, N, 0, 1));  // e^{+2 pi i j1 c / N}
-        }
-        reg_fft<4>(y, +1.0);
+            for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < L ? bh_get(bh + rd.bh_off, L, q0 + u * bd, 1) : make_double2(0.0, 0.0);
 #pragma unroll
-        for (int j2 = 0; j2 < 4; ++j2) {
-            outQ[j1 + qn * j2] = y[j2].x;
-            if (SPIN) outU[j1 + qn * j2] = y[j2].y;
+            for (int u = 0; u < kU; ++u)
+                if (q0 + u * bd < L) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
         }
+        __syncthreads();
+    }
+    fft_stockham_sm(buf, L, +1.0, T);
+    for (int j = threadIdx.x; j < Lq; j += bd) {
+        double2 v = buf[pidx(j)];
+        if (split) v = cmul(v, cis_pi((int)(((long long)j * j) % (2 * Lq)), Lq, 0, 1));
+        outQ[(size_t)Q * j + s] = v.x;
+        if (SPIN) outU[(size_t)Q * j + s] = v.y;
     }
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kBigThreads, 1) ring_adjoint_big_kernel(const int *__restrict__ ring_list,
-                                                                          const RingDesc *__restrict__ rings, int lmax,
-                                                                          int M, int nrings, long long npix,
-                                                                          const double *__restrict__ maps_all,
-                                                                          double2 *__restrict__ V_all,
-                                                                          const double2 *__restrict__ bh) {
-    extern __shared__ double2 sm[];
-    double2 *T = sm, *buf = sm + kBigBufOff;
-    const int r = ring_list[blockIdx.x];
+__global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_piece_kernel(const int *__restrict__ piece_list,
+                                                                             const RingDesc *__restrict__ rings, int lmax,
+                                                                             int M, int nrings, long long npix,
+                                                                             const double *__restrict__ maps_all,
+                                                                             double2 *__restrict__ V_all,
+                                                                             const double2 *__restrict__ tw,
+                                                                             const double2 *__restrict__ bh) {
+    extern __shared__ double2 buf[];
+    double2 *T = buf + kFftBufLen;  // twiddle table after the FFT buffer
+    sm_tw_init(T);
+    const int code = piece_list[blockIdx.x];
+    const int r = code >> 3, s = code & 7;
     const RingDesc rd = rings[r];
-    const int N = rd.N;
+    const int N = rd.N, Q = ring_pieces(rd), Lq = N / Q;
+    const bool split = rd.mode == kSplit4;
     const bool shifted = rd.phi0 != 0.0;
     constexpr int nchan = SPIN ? 2 : 1;
     const double *inQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
@@ -801,56 +833,83 @@ __global__ void __launch_bounds__(kBigThreads, 1) ring_adjoint_big_kernel(const 
     double2 *Vp = V_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     double2 *Vm = SPIN ? Vp + (size_t)nrings * M : Vp;
     const int bd = blockDim.x;
-    big_tw_init(T);
-    const bool direct = rd.mode == kDirect;
-    double2 *D = direct ? buf : sm + kBigDOff;
-    for (int j0 = threadIdx.x; j0 < N; j0 += kU * bd) {
-        double2 a[kU];
+    // b_s[j1]: the Q pixels j1 + Lq j2 with e^{-2 pi i s j / N}
+    for (int j10 = threadIdx.x; j10 < Lq; j10 += kU * bd) {
+        double2 acc[kU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int j = j0 + u * bd;
-            a[u] = j < N ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
-        }
+        for (int u = 0; u < kU; ++u) acc[u] = make_double2(0.0, 0.0);
+        double2 a[kMaxPieces][kU];  // every load issued before the first is used
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int j = j0 + u * bd;
-            if (j < N) D[direct ? pidx(j) : j] = a[u];
-        }
-    }
-    __syncthreads();
-    if (direct) {
-        fft_big(buf, N, -1.0, T);
-        gather_adjoint<SPIN, true>(buf, N, lmax, shifted, Vp, Vm);
-        return;
-    }
-    const int qn = N / 4;
-    for (int c = 0; c < 4; ++c) big_quarter_dft(D, buf, qn, c, rd.P, bh + rd.bh_off, -1, T);
-    // radix-4 combination in place: every thread holds its columns' four values first
-    constexpr int KM = (kBigN / 4 + kBigThreads - 1) / kBigThreads;
-    double2 y[KM][4];
+        for (int j2 = 0; j2 < kMaxPieces; ++j2)
 #pragma unroll
-    for (int u = 0; u < KM; ++u) {
-        const int k1 = threadIdx.x + u * kBigThreads;
-        if (k1 < qn) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                y[u][c] = D[4 * k1 + c];
-                if (c) y[u][c] = cmul(y[u][c], cis_pi(-2 * k1 * c, N, 0, 1));  // e^{-2 pi i k1 c / N}
+            for (int u = 0; u < kU; ++u) {
+                const int j = j10 + u * bd + Lq * j2;
+                a[j2][u] = (j2 < Q && j10 + u * bd < Lq) ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
             }
-            reg_fft<4>(y[u], -1.0);
+#pragma unroll
+        for (int j2 = 0; j2 < kMaxPieces; ++j2) {
+            if (j2 >= Q) break;
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int j1 = j10 + u * bd;
+                // power of two: e^{-2 pi i s j / N} from the table; kSplit4: its j2 part
+                // e^{-2 pi i s j2 / 4} (exact), the j1 part below
+                const double2 w = split ? root8(-2 * s * j2) : tw_pi(tw, -2LL * s * (j1 + Lq * j2), N);
+                acc[u] = cadd(acc[u], cmul(a[j2][u], w));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int j1 = j10 + u * bd;
+            if (j1 >= Lq) continue;
+            double2 v = acc[u];
+            // kSplit4: e^{-2 pi i s j1 / N} times the chirp conj(w(j1)) = e^{-i pi 4 j1^2 / N}
+            if (split) v = cmul(v, cis_pi(-(int)(((long long)2 * s * j1 + 4LL * j1 * j1) % (2LL * N)), N, 0, 1));
+            buf[pidx(j1)] = v;
         }
     }
+    const int L = split ? rd.P : Lq;
+    for (int k = Lq + threadIdx.x; k < L; k += bd) buf[pidx(k)] = make_double2(0.0, 0.0);
     __syncthreads();
+    fft_stockham_sm(buf, L, -1.0, T);
+    if (split) {  // W[k] = conj(w(k)) sum_j (b[j] conj(w(j))) w(k - j)
+        for (int q0 = threadIdx.x; q0 < L; q0 += kU * bd) {
+            double2 w[kU];
 #pragma unroll
-    for (int u = 0; u < KM; ++u) {
-        const int k1 = threadIdx.x + u * kBigThreads;
-        if (k1 < qn) {
+            for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < L ? bh_get(bh + rd.bh_off, L, q0 + u * bd, -1) : make_double2(0.0, 0.0);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) D[k1 + qn * c] = y[u][c];
+            for (int u = 0; u < kU; ++u)
+                if (q0 + u * bd < L) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
+        }
+        __syncthreads();
+        fft_stockham_sm(buf, L, +1.0, T);
+        for (int k = threadIdx.x; k < Lq; k += bd)
+            buf[pidx(k)] = cmul(buf[pidx(k)], cis_pi(-(int)(((long long)k * k) % (2 * Lq)), Lq, 0, 1));
+        __syncthreads();
+    }
+    // V rows: Vp[m] = W[m mod N] for m = s (mod Q), Vm[m] = conj(W[-m mod N]) for m = -s (mod Q),
+    // both times e^{-i m phi0} (gather_adjoint, restricted to this piece's residue class)
+    const int sm = (Q - s) % Q;
+    for (int m0 = threadIdx.x * Q; m0 <= lmax; m0 += kU * bd * Q) {
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int mp = m0 + u * bd * Q + s;  // Vp orders
+            if (mp <= lmax) {
+                double2 p = buf[pidx((mp % N - s) / Q)];
+                if (shifted) p = cmul(p, split ? cis_pi(-(mp % (2 * N)), N, 0, 1) : tw_pi(tw, -(long long)mp, N));
+                Vp[mp] = p;
+            }
+            if (SPIN) {
+                const int mm = m0 + u * bd * Q + sm;  // Vm orders
+                if (mm <= lmax) {
+                    const int k = (N - mm % N) % N;
+                    double2 q = conjd(buf[pidx((k - s) / Q)]);
+                    if (shifted) q = cmul(q, split ? cis_pi(-(mm % (2 * N)), N, 0, 1) : tw_pi(tw, -(long long)mm, N));
+                    Vm[mm] = q;
+                }
+            }
         }
     }
-    __syncthreads();
-    gather_adjoint<SPIN, false>(D, N, lmax, shifted, Vp, Vm);
 }
 
 // One block per (Bluestein length, piece): Bh+[Q q + s] = (1/P) sum_n b[n] e^{-2 pi i (Qq+s) n / P}.
@@ -891,16 +950,11 @@ __global__ void __launch_bounds__(kFftThreads) bluestein_setup_kernel(const int 
 }
 
 int smem_bytes() { return kFftBufLen * (int)sizeof(double2); }
+int smem_bytes_piece() { return (kFftBufLen + kSmTwLen) * (int)sizeof(double2); }
 
 template <typename K>
-int ensure_smem(K kernel) {
-    JHTB_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes()));
-    return JHTB_OK;
-}
-
-template <typename K>
-int ensure_smem_big(K kernel) {
-    JHTB_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBigSmem));
+int ensure_smem(K kernel, int bytes = smem_bytes()) {
+    JHTB_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     return JHTB_OK;
 }
 
@@ -913,10 +967,10 @@ int launch_ring_synth_t(const Plan &p, const double2 *F, double *maps, int nb, c
             p.d_ring_small, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F, maps, p.d_W, p.d_W2, p.d_tw, p.d_bh);
         JHTB_CUDA_TRY(cudaGetLastError());
     }
-    if (p.nring_big > 0) {
-        if ((rc = ensure_smem_big(ring_synth_big_kernel<SPIN>))) return rc;
-        ring_synth_big_kernel<SPIN><<<dim3(p.nring_big, nb), kBigThreads, kBigSmem, s>>>(
-            p.d_ring_big, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F, maps, p.d_bh);
+    if (p.nring_piece > 0) {
+        if ((rc = ensure_smem(ring_synth_piece_kernel<SPIN>, smem_bytes_piece()))) return rc;
+        ring_synth_piece_kernel<SPIN><<<dim3(p.nring_piece, nb), kFftThreads, smem_bytes_piece(), s>>>(
+            p.d_ring_piece, p.d_rings, p.lmax, p.M, p.nrings, p.npix, F, maps, p.d_tw, p.d_bh);
         JHTB_CUDA_TRY(cudaGetLastError());
     }
     return JHTB_OK;
@@ -931,10 +985,10 @@ int launch_ring_adjoint_t(const Plan &p, const double *maps, double2 *V, double2
             p.d_ring_small, p.d_rings, p.lmax, p.M, p.nrings, p.npix, maps, V, p.d_W2, W, p.d_tw, p.d_bh);
         JHTB_CUDA_TRY(cudaGetLastError());
     }
-    if (p.nring_big > 0) {
-        if ((rc = ensure_smem_big(ring_adjoint_big_kernel<SPIN>))) return rc;
-        ring_adjoint_big_kernel<SPIN><<<dim3(p.nring_big, nb), kBigThreads, kBigSmem, s>>>(
-            p.d_ring_big, p.d_rings, p.lmax, p.M, p.nrings, p.npix, maps, V, p.d_bh);
+    if (p.nring_piece > 0) {
+        if ((rc = ensure_smem(ring_adjoint_piece_kernel<SPIN>, smem_bytes_piece()))) return rc;
+        ring_adjoint_piece_kernel<SPIN><<<dim3(p.nring_piece, nb), kFftThreads, smem_bytes_piece(), s>>>(
+            p.d_ring_piece, p.d_rings, p.lmax, p.M, p.nrings, p.npix, maps, V, p.d_tw, p.d_bh);
         JHTB_CUDA_TRY(cudaGetLastError());
     }
     return JHTB_OK;
