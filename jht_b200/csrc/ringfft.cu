@@ -755,8 +755,9 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_piece_k
         double2 acc[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u) acc[u] = make_double2(0.0, 0.0);
-        // every load of the kU x Q terms is issued before the first is used
-        double2 d[kMaxPieces][kU];
+        // every load of the kU x Q terms (and, for a power of two, of the kU twiddles) is
+        // issued before the first is used
+        double2 d[kMaxPieces][kU], w1[kU];
 #pragma unroll
         for (int k2 = 0; k2 < kMaxPieces; ++k2)
 #pragma unroll
@@ -765,24 +766,27 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_piece_k
                 d[k2][u] = (k2 < Q && k1 < Lq) ? fold_one(Fp, Fm, k1 + Lq * k2, N, lmax, shifted) : make_double2(0.0, 0.0);
             }
 #pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int k1 = k10 + u * bd;
+            w1[u] = (!split && k1 < Lq) ? tw_pi(tw, (long long)c * k1, N) : make_double2(1.0, 0.0);
+        }
+        // e^{i pi c (k1 + Lq k2) / N} = e^{i pi c k1 / N} e^{i pi c k2 / Q}: the k2 factor is an
+        // eighth root of unity (exactly +-1, +-i for Q = 2), the k1 factor is applied once
+#pragma unroll
         for (int k2 = 0; k2 < kMaxPieces; ++k2) {
             if (k2 >= Q) break;
+            const double2 w = root8((4 / Q) * c * k2);
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const int k1 = k10 + u * bd;
-                // power of two: e^{i pi c k / N} exactly from the table; kSplit4: the k2 part of
-                // e^{i pi c (k1 + Lq k2) / N} = e^{i pi c k1 / N} e^{i pi c k2 / 4} (the k1 part below)
-                const double2 w = split ? root8(c * k2) : tw_pi(tw, (long long)c * (k1 + Lq * k2), N);
-                acc[u] = cadd(acc[u], cmul(d[k2][u], w));
-            }
+            for (int u = 0; u < kU; ++u) acc[u] = cadd(acc[u], k2 ? cmul(d[k2][u], w) : d[k2][u]);
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const int k1 = k10 + u * bd;
             if (k1 >= Lq) continue;
-            double2 v = acc[u];
-            // kSplit4: e^{i pi c k1 / N} times the chirp w(k1) = e^{i pi k1^2 / Lq} = e^{i pi 4 k1^2 / N}
-            if (split) v = cmul(v, cis_pi((int)(((long long)c * k1 + 4LL * k1 * k1) % (2LL * N)), N, 0, 1));
+            // power of two: e^{i pi c k1 / N} from the table; kSplit4: e^{i pi c k1 / N} times the
+            // chirp w(k1) = e^{i pi k1^2 / Lq} = e^{i pi 4 k1^2 / N}, one exactly reduced argument
+            const double2 v = split ? cmul(acc[u], cis_pi((int)(((long long)c * k1 + 4LL * k1 * k1) % (2LL * N)), N, 0, 1))
+                                    : cmul(acc[u], w1[u]);
             buf[pidx(k1)] = v;
         }
     }
@@ -838,7 +842,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_piece
         double2 acc[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u) acc[u] = make_double2(0.0, 0.0);
-        double2 a[kMaxPieces][kU];  // every load issued before the first is used
+        double2 a[kMaxPieces][kU], w1[kU];  // every load issued before the first is used
 #pragma unroll
         for (int j2 = 0; j2 < kMaxPieces; ++j2)
 #pragma unroll
@@ -847,24 +851,27 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_piece
                 a[j2][u] = (j2 < Q && j10 + u * bd < Lq) ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
             }
 #pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int j1 = j10 + u * bd;
+            w1[u] = (!split && j1 < Lq) ? tw_pi(tw, -2LL * s * j1, N) : make_double2(1.0, 0.0);
+        }
+        // e^{-2 pi i s (j1 + Lq j2) / N} = e^{-2 pi i s j1 / N} e^{-2 pi i s j2 / Q}: the j2 factor
+        // is a fourth root of unity (exact), the j1 factor is applied once
+#pragma unroll
         for (int j2 = 0; j2 < kMaxPieces; ++j2) {
             if (j2 >= Q) break;
+            const double2 w = root8(-(8 / Q) * s * j2);
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const int j1 = j10 + u * bd;
-                // power of two: e^{-2 pi i s j / N} from the table; kSplit4: its j2 part
-                // e^{-2 pi i s j2 / 4} (exact), the j1 part below
-                const double2 w = split ? root8(-2 * s * j2) : tw_pi(tw, -2LL * s * (j1 + Lq * j2), N);
-                acc[u] = cadd(acc[u], cmul(a[j2][u], w));
-            }
+            for (int u = 0; u < kU; ++u) acc[u] = cadd(acc[u], j2 ? cmul(a[j2][u], w) : a[j2][u]);
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const int j1 = j10 + u * bd;
             if (j1 >= Lq) continue;
-            double2 v = acc[u];
-            // kSplit4: e^{-2 pi i s j1 / N} times the chirp conj(w(j1)) = e^{-i pi 4 j1^2 / N}
-            if (split) v = cmul(v, cis_pi(-(int)(((long long)2 * s * j1 + 4LL * j1 * j1) % (2LL * N)), N, 0, 1));
+            // power of two: e^{-2 pi i s j1 / N} from the table; kSplit4: times the chirp
+            // conj(w(j1)) = e^{-i pi 4 j1^2 / N}, one exactly reduced argument
+            const double2 v = split ? cmul(acc[u], cis_pi(-(int)(((long long)2 * s * j1 + 4LL * j1 * j1) % (2LL * N)), N, 0, 1))
+                                    : cmul(acc[u], w1[u]);
             buf[pidx(j1)] = v;
         }
     }
