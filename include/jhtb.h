@@ -255,6 +255,15 @@ int jhtb_plan_set_tuning(jhtb_plan *plan, int key, int value);
 #define JHTB_FAULT_STALL 1
 int jhtb_plan_inject_fault(jhtb_plan *plan, int kind);
 
+/* Bounds-check record of a debug library (no counterpart in jht; the replacement for a
+ * memory checker on machines where none can run).  A library built with `make debug`
+ * (jht_b200/_lib_debug/libjhtb.so, -DJHTB_DEBUG) tests every checked gather and scatter
+ * index of its kernels against the extent of its buffer and skips an access out of range;
+ * this call waits for the device, returns the number of such accesses since the last call
+ * and the first one's site code, index and extent, and clears the record.  The release
+ * library compiles no checks and returns JHTB_ERR_UNSUPPORTED. */
+int jhtb_debug_bounds(int64_t *count, int *site, int64_t *index, int64_t *extent);
+
 /* FP64 FMA throughput probe: a grid of 148*blocks_per_sm CTAs x 256 threads, each
  * running 8 independent FMA chains for `iters` steps.  Writes the elapsed time of
  * the launch (CUDA events on `stream`) to *ms and the FLOP count (2 per FMA) to

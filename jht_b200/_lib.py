@@ -55,6 +55,7 @@ EXPORTS = (
     "jhtb_nufft_interp",
     "jhtb_nufft_spread",
     "jhtb_nufft_spread_tiles",
+    "jhtb_debug_bounds",
 )
 
 
@@ -121,6 +122,8 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_nufft_spread": (i32, [vp, dp, dp, i64, i32, i32, i32, ctypes.c_double, vp, vp]),
             "jhtb_nufft_spread_tiles": (i32, [vp, dp, dp, i64, i64, vp, vp, vp, i32, i32, i32, i32, ctypes.c_double,
                                               vp, vp]),
+            "jhtb_debug_bounds": (i32, [ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i64),
+                                        ctypes.POINTER(i64)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -129,6 +132,20 @@ def load_library(path: str | os.PathLike | None = None):
         if path is None:
             _lib = lib
         return lib
+
+
+DEBUG_LIB_PATH = LIB_PATH.parent.parent / "_lib_debug" / "libjhtb.so"
+
+
+def debug_bounds(lib=None) -> dict:
+    """The bounds-check record of a debug library (``make debug``): failed accesses since
+    the last call, with the first one's site code, index and extent (clears the record).
+    Raises JhtbError (status JHTB_ERR_UNSUPPORTED) on the release library."""
+    lib = lib or load_library()
+    cnt, site, idx, ext = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+    check(lib.jhtb_debug_bounds(ctypes.byref(cnt), ctypes.byref(site), ctypes.byref(idx), ctypes.byref(ext)),
+          "jhtb_debug_bounds")
+    return {"count": cnt.value, "site": site.value, "index": idx.value, "extent": ext.value}
 
 
 def last_error() -> str:

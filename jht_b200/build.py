@@ -14,16 +14,20 @@ from pathlib import Path
 CSRC = Path(__file__).resolve().parent / "csrc"
 
 
-def build(jobs: int = 4, verbose: bool = False) -> Path:
+def build(jobs: int = 4, verbose: bool = False, debug: bool = False) -> Path:
+    """Build the release library; with ``debug`` the bounds-checked one instead
+    (``jht_b200/_lib_debug/libjhtb.so``, every checked index reported by jhtb_debug_bounds)."""
     cmd = ["make", "-C", str(CSRC), f"-j{jobs}"]
+    if debug:
+        cmd.append("debug")
     if not verbose:
         cmd.append("-s")
     subprocess.run(cmd, check=True, env=dict(os.environ))
-    lib = CSRC.parent / "_lib" / "libjhtb.so"
+    lib = CSRC.parent / ("_lib_debug" if debug else "_lib") / "libjhtb.so"
     if not lib.exists():
         raise RuntimeError(f"build finished but {lib} is missing")
     return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    print(build(verbose="-v" in sys.argv, debug="--debug" in sys.argv))

@@ -255,4 +255,51 @@ __host__ __device__ inline long long alm_index(long long l, long long m, long lo
     return m * (2 * lmax + 1 - m) / 2 + l;
 }
 
+// ---------------------------------------------------------------------------------
+// Debug bounds checks (a library built with -DJHTB_DEBUG: `make debug`).  Every checked
+// gather or scatter tests its index against the extent of its buffer; an access out of
+// range is skipped (a load reads zero), and the number of failures with the first one's
+// site, index and extent is kept in a device record per translation unit, which
+// jhtb_debug_bounds() collects.  Without JHTB_DEBUG a check is the constant true and the
+// access is unchanged.  Site numbers: 1xx azimuthal stage, 2xx FP64 Legendre kernels,
+// 3xx tensor-core synthesis, 4xx tensor-core adjoint, 5xx vector kernels.
+// ---------------------------------------------------------------------------------
+struct DebugRecord {
+    unsigned long long count;
+    long long index, extent;
+    int site, pad;
+};
+#ifdef JHTB_DEBUG
+static __device__ DebugRecord g_debug_record;
+__device__ __forceinline__ bool debug_in_range(long long i, long long n, int site) {
+    if (i >= 0 && i < n) return true;
+    if (atomicAdd(&g_debug_record.count, 1ull) == 0ull) {
+        g_debug_record.site = site;
+        g_debug_record.index = i;
+        g_debug_record.extent = n;
+    }
+    return false;
+}
+#define JHTB_IN(i, n, site) ::jhtb::debug_in_range((long long)(i), (long long)(n), (site))
+// the record of this translation unit: copied out and, with reset, cleared
+#define JHTB_DEBUG_ACCESSOR(name)                                                            \
+    int debug_record_##name(::jhtb::DebugRecord *out, bool reset) {                          \
+        if (cudaMemcpyFromSymbol(out, g_debug_record, sizeof(::jhtb::DebugRecord)) != cudaSuccess) \
+            return 1;                                                                         \
+        if (reset) {                                                                          \
+            const ::jhtb::DebugRecord z{};                                                    \
+            if (cudaMemcpyToSymbol(g_debug_record, &z, sizeof(z)) != cudaSuccess) return 1;   \
+        }                                                                                     \
+        return 0;                                                                             \
+    }
+#else
+#define JHTB_IN(i, n, site) true
+#define JHTB_DEBUG_ACCESSOR(name)
+#endif
+int debug_record_legendre(DebugRecord *out, bool reset);
+int debug_record_ringfft(DebugRecord *out, bool reset);
+int debug_record_tc_synth(DebugRecord *out, bool reset);
+int debug_record_tc_adjoint(DebugRecord *out, bool reset);
+int debug_record_vecops(DebugRecord *out, bool reset);
+
 }  // namespace jhtb

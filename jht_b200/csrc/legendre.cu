@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth0_kernel(LegParams p
         }
         for (int i0 = i_start; i0 < nst; i0 += kStage) {
             const int cnt = min(kStage, nst - i0);
-            if (lane < cnt) {
+            if (lane < cnt && JHTB_IN(b0 + i0 + lane, p.K, 201)) {
                 const long long idx = b0 + i0 + lane;
                 const double c = p.cnorm[idx];
                 const double2 a = alm[idx];
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth0_kernel(LegParams p
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int t = tile * 32 * R + r * 32 + lane;
-            if (t < p.T) {
+            if (t < p.T && JHTB_IN((long long)(p.nrings - 1 - t) * p.M + m, (long long)p.nrings * p.M, 202)) {
                 F[(size_t)t * p.M + m] = make_double2(Ar[r] + Br[r], Ai[r] + Bi[r]);
                 if (t < p.T - 1)
                     F[(size_t)(p.nrings - 1 - t) * p.M + m] = make_double2(Ar[r] - Br[r], Ai[r] - Bi[r]);
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth2_kernel(LegParams p
         }
         for (int i0 = i_start; i0 < nst; i0 += kStage) {
             const int cnt = min(kStage, nst - i0);
-            if (lane < cnt) {
+            if (lane < cnt && JHTB_IN(b0 + i0 + lane, p.K, 201)) {
                 const long long idx = b0 + i0 + lane;
                 const double c = p.cnorm[idx];
                 const double2 e = aE[idx], bb = aB[idx];
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) synth2_kernel(LegParams p
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int t = tile * 32 * R + r * 32 + lane;
-            if (t < p.T) {
+            if (t < p.T && JHTB_IN((long long)(p.nrings - 1 - t) * p.M + m, (long long)p.nrings * p.M, 202)) {
                 const Acc2 &a = acc[r];
                 Fp[(size_t)t * p.M + m] = make_double2(a.ppr, a.ppi);
                 Fm[(size_t)t * p.M + m] = make_double2(a.mmr, a.mmi);
@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj0MinBlocks) adj0_kern
                 const int t = tile * 32 * R + r * 32 + lane;
                 double2 vn = make_double2(0.0, 0.0), vs = make_double2(0.0, 0.0);
                 x[r] = 0.0;
-                if (t < p.T) {
+                if (t < p.T && JHTB_IN((long long)(p.nrings - 1 - t) * p.M + m, (long long)p.nrings * p.M, 203)) {
                     x[r] = p.x[t];
                     vn = V[(size_t)t * p.M + m];
                     if (t < p.T - 1) vs = V[(size_t)(p.nrings - 1 - t) * p.M + m];
@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj0MinBlocks) adj0_kern
                     const int qw = q0 + lane / LPE;
                     const bool wr = (lane % LPE) == 0 && qw < cnt;
                     double2 prev = make_double2(0.0, 0.0);
-                    if (acc && wr) prev = part[b0 + i0 + qw];
+                    if (acc && wr && JHTB_IN(b0 + i0 + qw, p.K, 204)) prev = part[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
 #pragma unroll
                     for (int q = 0; q < kSub; q += 2) {
@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj0MinBlocks) adj0_kern
                     __syncwarp();
                     const double2 tot = red_sum<kSub>(rb, lane);
                     __syncwarp();
-                    if (wr) part[b0 + i0 + qw] = make_double2(tot.x + prev.x, tot.y + prev.y);
+                    if (wr && JHTB_IN(b0 + i0 + qw, p.K, 204)) part[b0 + i0 + qw] = make_double2(tot.x + prev.x, tot.y + prev.y);
                 }
                 __syncwarp();
             }
@@ -720,7 +720,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj2MinBlocks) adj2_kern
                 In2 d;
                 d.vpn = d.spA = d.vmn = d.smA = make_double2(0.0, 0.0);
                 x[r] = 0.0;
-                if (t < p.T) {
+                if (t < p.T && JHTB_IN((long long)(p.nrings - 1 - t) * p.M + m, (long long)p.nrings * p.M, 203)) {
                     x[r] = p.x[t];
                     d.vpn = Vp[(size_t)t * p.M + m];
                     d.vmn = Vm[(size_t)t * p.M + m];
@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj2MinBlocks) adj2_kern
                     const bool wr = (lane % LPE) == 0 && qw < cnt;
                     double2 *dstw = e >= kSub ? partM : partP;
                     double2 prev = make_double2(0.0, 0.0);
-                    if (acc && wr) prev = dstw[b0 + i0 + qw];
+                    if (acc && wr && JHTB_IN(b0 + i0 + qw, p.K, 204)) prev = dstw[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
 #pragma unroll
                     for (int q = 0; q < kSub; q += 2) {
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj2MinBlocks) adj2_kern
                     __syncwarp();
                     const double2 tot = red_sum<NV>(rb, lane);
                     __syncwarp();
-                    if (wr) dstw[b0 + i0 + qw] = make_double2(tot.x + prev.x, tot.y + prev.y);
+                    if (wr && JHTB_IN(b0 + i0 + qw, p.K, 204)) dstw[b0 + i0 + qw] = make_double2(tot.x + prev.x, tot.y + prev.y);
                 }
                 __syncwarp();
             }
@@ -795,6 +795,7 @@ __global__ void adj_reduce_kernel(int lmax, long long K, int nsuper, const SeedP
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
         const int b = (int)(g / K);
         const long long idx = g - (long long)b * K;
+        if (!JHTB_IN(idx, K, 205)) continue;
         // (l, m) of the packed index: m from the column base
         int m = (int)floor(((2.0 * lmax + 3.0) - sqrt((2.0 * lmax + 3.0) * (2.0 * lmax + 3.0) - 8.0 * (double)idx)) / 2.0);
         if (m < 0) m = 0;
@@ -852,6 +853,8 @@ int leg_grid(const Plan &p, Kern k) {
 }
 
 }  // namespace
+
+JHTB_DEBUG_ACCESSOR(legendre)
 
 int launch_start_states(const Plan &p, cudaStream_t s) {
     const int nitems = p.M * p.ntiles;

@@ -905,6 +905,31 @@ int jhtb_plan_inject_fault(jhtb_plan *plan, int kind) {
     return JHTB_OK;
 }
 
+int jhtb_debug_bounds(int64_t *count, int *site, int64_t *index, int64_t *extent) {
+    if (!count || !site || !index || !extent) return fail(JHTB_ERR_INVALID, "jhtb_debug_bounds: NULL argument");
+    *count = 0;
+    *site = 0;
+    *index = *extent = 0;
+#ifdef JHTB_DEBUG
+    JHTB_CUDA_TRY(cudaDeviceSynchronize());
+    int (*const readers[])(DebugRecord *, bool) = {debug_record_legendre, debug_record_ringfft, debug_record_tc_synth,
+                                                   debug_record_tc_adjoint, debug_record_vecops};
+    for (auto rd : readers) {
+        DebugRecord r{};
+        if (rd(&r, true)) return fail(JHTB_ERR_CUDA, "jhtb_debug_bounds: reading a bounds record failed");
+        if (r.count && !*count) {
+            *site = r.site;
+            *index = r.index;
+            *extent = r.extent;
+        }
+        *count += (int64_t)r.count;
+    }
+    return JHTB_OK;
+#else
+    return fail(JHTB_ERR_UNSUPPORTED, "jhtb_debug_bounds: bounds checks are compiled into the debug library only (make debug)");
+#endif
+}
+
 int jhtb_plan_ring_costs(const jhtb_plan *plan, int granule, int64_t *cost, int ncost) {
     if (!plan || !cost) return fail(JHTB_ERR_INVALID, "jhtb_plan_ring_costs: NULL argument");
     const Plan &p = *reinterpret_cast<const Plan *>(plan);

@@ -76,7 +76,7 @@ __device__ __forceinline__ double2 root(long long a, long long b, double sgn) {
 // dividing kTwLen; `plus` selects the + sign.
 __device__ __forceinline__ double2 twid(const double2 *__restrict__ tw, int a, int L, bool plus) {
     int r = a & (L - 1);
-    double2 w = __ldg(&tw[r * (kTwLen / L)]);
+    double2 w = JHTB_IN(r * (kTwLen / L), kTwLen, 107) ? __ldg(&tw[r * (kTwLen / L)]) : make_double2(0.0, 0.0);
     if (plus) w.y = -w.y;
     return w;
 }
@@ -167,7 +167,7 @@ __device__ __forceinline__ void stockham_pass(double2 *buf, int n, int Ns, doubl
                 const int step = jm * (kTwLen / (Ns * R));
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    double2 w = __ldg(&tw[step * r]);
+                    double2 w = JHTB_IN(step * r, kTwLen, 107) ? __ldg(&tw[step * r]) : make_double2(0.0, 0.0);
                     if (dir > 0) w.y = -w.y;
                     v[jj][r] = cmul(v[jj][r], w);
                 }
@@ -276,6 +276,7 @@ __device__ __forceinline__ void fft_stockham_sm(double2 *buf, int n, double dir,
 // b[n] = conj(w(n)) on |n| < N, w(n) = e^{+i pi n^2 / N}.  The adjoint direction
 // uses Bh-[k] = conj(Bh+[(P - k) mod P]).
 __device__ __forceinline__ double2 bh_get(const double2 *bh, int P, int k, int sgn) {
+    if (!JHTB_IN(k, P, 108)) return make_double2(0.0, 0.0);
     if (sgn > 0) return __ldg(&bh[k]);
     return conjd(__ldg(&bh[(P - k) & (P - 1)]));
 }
@@ -294,7 +295,7 @@ __device__ __forceinline__ double2 fold_synth(const double2 *__restrict__ Fp, co
     const int step = parts * N;
 #pragma unroll 4
     for (int m = k + part * N; m <= lmax; m += step) {
-        const double2 f = Fp[m];
+        const double2 f = JHTB_IN(m, lmax + 1, 101) ? Fp[m] : make_double2(0.0, 0.0);
         d.x = fma(sg, f.x, d.x);
         d.y = fma(sg, f.y, d.y);
         sg *= flip;
@@ -303,7 +304,7 @@ __device__ __forceinline__ double2 fold_synth(const double2 *__restrict__ Fp, co
     sg = (shifted && ((1 + part) & 1)) ? -1.0 : 1.0;
 #pragma unroll 4
     for (int m = (1 + part) * N - k; m <= lmax; m += step) {
-        const double2 f = Fm[m];
+        const double2 f = JHTB_IN(m, lmax + 1, 102) ? Fm[m] : make_double2(0.0, 0.0);
         d.x = fma(sg, f.x, d.x);
         d.y = fma(-sg, f.y, d.y);
         sg *= flip;
@@ -334,8 +335,8 @@ __device__ __forceinline__ void synth_fold(const double2 *__restrict__ Fp, const
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int k = k0 + u * blockDim.x;
-                fp[u] = (k < N && k <= lmax) ? Fp[k] : make_double2(0.0, 0.0);
-                fm[u] = (k < N && k >= 1 && N - k <= lmax) ? Fm[N - k] : make_double2(0.0, 0.0);
+                fp[u] = (k < N && k <= lmax && JHTB_IN(k, lmax + 1, 101)) ? Fp[k] : make_double2(0.0, 0.0);
+                fm[u] = (k < N && k >= 1 && N - k <= lmax && JHTB_IN(N - k, lmax + 1, 102)) ? Fm[N - k] : make_double2(0.0, 0.0);
             }
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
@@ -414,8 +415,10 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
         for (int j = threadIdx.x; j < N; j += bd) {
             double2 v = buf[pidx(j)];
             if (blue) v = cmul(v, cis_pi((int)(((long long)j * j) % (2 * N)), N, 0, 1));
-            outQ[j] = v.x;
-            if (SPIN) outU[j] = v.y;
+            if (JHTB_IN(rd.start + j, npix, 104)) {
+                outQ[j] = v.x;
+                if (SPIN) outU[j] = v.y;
+            }
         }
         return;
     }
@@ -438,7 +441,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
                 for (int u = 0; u < kU; ++u) {
                     const int k = q0 + u * bd + t * Lp;
                     const bool ok = q0 + u * bd < Lp && k < N;
-                    a[u] = ok ? Ag[k] : make_double2(0.0, 0.0);
+                    a[u] = (ok && JHTB_IN(rd.start + k, npix, 109)) ? Ag[k] : make_double2(0.0, 0.0);
                     // direct: inverse DFT, e^{+2 pi i s k / N}; chirp-z: FFT_P, e^{-2 pi i s k / P}
                     w[u] = (ok && s) ? twid(tw, s * k, L, !blue) : make_double2(1.0, 0.0);
                 }
@@ -454,8 +457,10 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
             fft_stockham(buf, Lp, +1.0, tw);
             for (int q = threadIdx.x; q < Lp; q += bd) {
                 const double2 v = buf[pidx(q)];
-                outQ[Q * q + s] = v.x;
-                if (SPIN) outU[Q * q + s] = v.y;
+                if (JHTB_IN(rd.start + (long long)Q * q + s, npix, 104)) {
+                    outQ[Q * q + s] = v.x;
+                    if (SPIN) outU[Q * q + s] = v.y;
+                }
             }
             __syncthreads();
             continue;
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int j = j0 + u * bd;
-                y[u] = (s && j < N) ? Yg[j] : make_double2(0.0, 0.0);
+                y[u] = (s && j < N && JHTB_IN(rd.start + j, npix, 109)) ? Yg[j] : make_double2(0.0, 0.0);
                 w[u] = (s && j < N) ? twid(tw, s * j, L, true) : make_double2(1.0, 0.0);
             }
 #pragma unroll
@@ -486,11 +491,13 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_kernel(
                 if (j >= N) continue;
                 double2 v = cadd(y[u], cmul(buf[pidx(j & (Lp - 1))], w[u]));
                 if (s < Q - 1) {
-                    Yg[j] = v;
+                    if (JHTB_IN(rd.start + j, npix, 109)) Yg[j] = v;
                 } else {
                     v = cmul(v, cis_pi((int)(((long long)j * j) % (2 * N)), N, 0, 1));
-                    outQ[j] = v.x;
-                    if (SPIN) outU[j] = v.y;
+                    if (JHTB_IN(rd.start + j, npix, 104)) {
+                        outQ[j] = v.x;
+                        if (SPIN) outU[j] = v.y;
+                    }
                 }
             }
         }
@@ -523,8 +530,10 @@ __device__ __forceinline__ void gather_adjoint(const double2 *W, int N, int lmax
                 p = cmul(p, cph);
                 q = cmul(q, cph);
             }
-            Vp[m] = p;
-            if (SPIN) Vm[m] = q;
+            if (JHTB_IN(m, lmax + 1, 105)) {
+                Vp[m] = p;
+                if (SPIN) Vm[m] = q;
+            }
         }
     }
 }
@@ -557,7 +566,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const int j = j0 + u * bd;
-            a[u] = j < N ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
+            a[u] = (j < N && JHTB_IN(rd.start + j, npix, 103)) ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
@@ -608,7 +617,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
             load_in(j0, a);
 #pragma unroll
             for (int u = 0; u < kU; ++u)
-                if (j0 + u * bd < N) Ag[j0 + u * bd] = a[u];
+                if (j0 + u * bd < N && JHTB_IN(rd.start + j0 + u * bd, npix, 109)) Ag[j0 + u * bd] = a[u];
         }
         __syncthreads();
     }
@@ -636,7 +645,8 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
         __syncthreads();
         fft_stockham(buf, Lp, -1.0, tw);
         if (!blue) {  // W[Q q + s]
-            for (int q = threadIdx.x; q < Lp; q += bd) Wg[Q * q + s] = buf[pidx(q)];
+            for (int q = threadIdx.x; q < Lp; q += bd)
+                if (JHTB_IN(rd.start + (long long)Q * q + s, npix, 109)) Wg[Q * q + s] = buf[pidx(q)];
             __syncthreads();
             continue;
         }
@@ -656,7 +666,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int k = k0 + u * bd;
-                y[u] = (s && k < N) ? Wg[k] : make_double2(0.0, 0.0);
+                y[u] = (s && k < N && JHTB_IN(rd.start + k, npix, 109)) ? Wg[k] : make_double2(0.0, 0.0);
                 w[u] = (s && k < N) ? twid(tw, s * k, L, true) : make_double2(1.0, 0.0);
             }
 #pragma unroll
@@ -665,7 +675,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
                 if (k >= N) continue;
                 double2 v = cadd(y[u], cmul(buf[pidx(k & (Lp - 1))], w[u]));
                 if (s == Q - 1) v = cmul(v, cis_pi(-(int)(((long long)k * k) % (2 * N)), N, 0, 1));
-                Wg[k] = v;
+                if (JHTB_IN(rd.start + k, npix, 109)) Wg[k] = v;
             }
         }
         __syncthreads();
@@ -692,7 +702,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_kerne
 // e^{-2 pi i j / kTwLen}, each rounded once).
 __device__ __forceinline__ double2 tw_pi(const double2 *__restrict__ tw, long long a, int N) {
     const int r = (int)(a & (2LL * N - 1));
-    double2 w = __ldg(&tw[r * (kTwLen / (2 * N))]);
+    double2 w = JHTB_IN(r * (kTwLen / (2 * N)), kTwLen, 107) ? __ldg(&tw[r * (kTwLen / (2 * N))]) : make_double2(0.0, 0.0);
     w.y = -w.y;
     return w;
 }
@@ -720,8 +730,8 @@ __device__ __forceinline__ double2 root8(int k) {
 __device__ __forceinline__ double2 fold_one(const double2 *__restrict__ Fp, const double2 *__restrict__ Fm, int k, int N,
                                             int lmax, bool shifted) {
     if (N <= lmax) return fold_synth(Fp, Fm, k, N, lmax, shifted);
-    const double2 fp = k <= lmax ? Fp[k] : make_double2(0.0, 0.0);
-    const double2 fm = (k >= 1 && N - k <= lmax) ? Fm[N - k] : make_double2(0.0, 0.0);
+    const double2 fp = (k <= lmax && JHTB_IN(k, lmax + 1, 101)) ? Fp[k] : make_double2(0.0, 0.0);
+    const double2 fm = (k >= 1 && N - k <= lmax && JHTB_IN(N - k, lmax + 1, 102)) ? Fm[N - k] : make_double2(0.0, 0.0);
     const double sg = shifted ? -1.0 : 1.0;
     return make_double2(fma(sg, fm.x, fp.x), fma(-sg, fm.y, fp.y));
 }
@@ -787,7 +797,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_piece_k
             // chirp w(k1) = e^{i pi k1^2 / Lq} = e^{i pi 4 k1^2 / N}, one exactly reduced argument
             const double2 v = split ? cmul(acc[u], cis_pi((int)(((long long)c * k1 + 4LL * k1 * k1) % (2LL * N)), N, 0, 1))
                                     : cmul(acc[u], w1[u]);
-            buf[pidx(k1)] = v;
+            if (JHTB_IN(pidx(k1), kFftBufLen, 106)) buf[pidx(k1)] = v;
         }
     }
     const int L = split ? rd.P : Lq;
@@ -809,8 +819,10 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_piece_k
     for (int j = threadIdx.x; j < Lq; j += bd) {
         double2 v = buf[pidx(j)];
         if (split) v = cmul(v, cis_pi((int)(((long long)j * j) % (2 * Lq)), Lq, 0, 1));
-        outQ[(size_t)Q * j + s] = v.x;
-        if (SPIN) outU[(size_t)Q * j + s] = v.y;
+        if (JHTB_IN(rd.start + (long long)Q * j + s, npix, 104)) {
+            outQ[(size_t)Q * j + s] = v.x;
+            if (SPIN) outU[(size_t)Q * j + s] = v.y;
+        }
     }
 }
 
@@ -848,7 +860,8 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_piece
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
                 const int j = j10 + u * bd + Lq * j2;
-                a[j2][u] = (j2 < Q && j10 + u * bd < Lq) ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
+                a[j2][u] = (j2 < Q && j10 + u * bd < Lq && JHTB_IN(rd.start + j, npix, 103)) ? make_double2(inQ[j], SPIN ? inU[j] : 0.0)
+                                                                                            : make_double2(0.0, 0.0);
             }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
@@ -872,7 +885,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_piece
             // conj(w(j1)) = e^{-i pi 4 j1^2 / N}, one exactly reduced argument
             const double2 v = split ? cmul(acc[u], cis_pi(-(int)(((long long)2 * s * j1 + 4LL * j1 * j1) % (2LL * N)), N, 0, 1))
                                     : cmul(acc[u], w1[u]);
-            buf[pidx(j1)] = v;
+            if (JHTB_IN(pidx(j1), kFftBufLen, 106)) buf[pidx(j1)] = v;
         }
     }
     const int L = split ? rd.P : Lq;
@@ -902,17 +915,19 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_piece
         for (int u = 0; u < kU; ++u) {
             const int mp = m0 + u * bd * Q + s;  // Vp orders
             if (mp <= lmax) {
-                double2 p = buf[pidx((mp % N - s) / Q)];
+                const int kp = (mp % N - s) / Q;
+                double2 p = JHTB_IN(kp, Lq, 106) ? buf[pidx(kp)] : make_double2(0.0, 0.0);
                 if (shifted) p = cmul(p, split ? cis_pi(-(mp % (2 * N)), N, 0, 1) : tw_pi(tw, -(long long)mp, N));
-                Vp[mp] = p;
+                if (JHTB_IN(mp, M, 105)) Vp[mp] = p;
             }
             if (SPIN) {
                 const int mm = m0 + u * bd * Q + sm;  // Vm orders
                 if (mm <= lmax) {
                     const int k = (N - mm % N) % N;
-                    double2 q = conjd(buf[pidx((k - s) / Q)]);
+                    const int kq = (k - s) / Q;
+                    double2 q = JHTB_IN(kq, Lq, 106) ? conjd(buf[pidx(kq)]) : make_double2(0.0, 0.0);
                     if (shifted) q = cmul(q, split ? cis_pi(-(mm % (2 * N)), N, 0, 1) : tw_pi(tw, -(long long)mm, N));
-                    Vm[mm] = q;
+                    if (JHTB_IN(mm, M, 105)) Vm[mm] = q;
                 }
             }
         }
@@ -1002,6 +1017,8 @@ int launch_ring_adjoint_t(const Plan &p, const double *maps, double2 *V, double2
 }
 
 }  // namespace
+
+JHTB_DEBUG_ACCESSOR(ringfft)
 
 int launch_ring_synth(const Plan &p, const double2 *F, double *maps, int nb, cudaStream_t s) {
     if (nb <= 0) return JHTB_OK;

@@ -296,6 +296,7 @@ __device__ void adj_loader(const AdjParams &p, AdjSmem<SPIN> &sm, int lane) {
             const int nstg = item_stages(q);
             const int cb = n & 1;
             const unsigned char *tiles = p.Bt + ((size_t)q.m * p.nchunk + q.c0) * kBStage;
+            (void)JHTB_IN(q.c0 + nstg - 1, p.nchunk, 402);  // the item's tiles lie inside its order's row
             for (int s = 0; s < min(kPrefetch, nstg); ++s) bulk_prefetch_l2(tiles + (size_t)s * kBStage, kBStage);
             if (n >= 2 && !mbar_wait(&sm.coefEmpty[cb], ((n >> 1) - 1u) & 1u, p.wait_ns)) {
                 ok = false;
@@ -488,10 +489,11 @@ __device__ void adj_epilogue(const AdjParams &p, AdjSmem<SPIN> &sm, double2 *__r
         // live rings); spin 2: E = (-p2 - m2) c / 2, B = i (p2 - m2) c / 2 (healpix.py:353-354)
         if (l <= p.lmax) {
             const long long idx = alm_index(l, q.m, p.lmax);
-            const double c = __ldg(&p.cnorm[idx]);
+            const bool in = JHTB_IN(idx, p.K, 401);
+            const double c = in ? __ldg(&p.cnorm[idx]) : 0.0;
 #pragma unroll
             for (int b = 0; b < kTcaMaps; ++b) {
-                if (b >= nb) continue;
+                if (b >= nb || !in) continue;
                 if (SPIN) {
                     const double pr = c * acc[4 * b + 0], pi = c * acc[4 * b + 1];
                     const double mr = c * acc[4 * b + 2], mi = c * acc[4 * b + 3];
@@ -680,6 +682,8 @@ __global__ void __launch_bounds__(128) tca_segment_state_kernel(int lmax, int T,
 }
 
 }  // namespace
+
+JHTB_DEBUG_ACCESSOR(tc_adjoint)
 
 int launch_tca_block_states(const Plan &p, cudaStream_t s) {
     const dim3 grid((p.T + 127) / 128, p.spin ? 2 : 1, p.M);

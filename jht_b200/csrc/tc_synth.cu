@@ -195,6 +195,7 @@ template <int SPIN>
 __device__ __forceinline__ void tc_store_F(const TcParams &p, double2 *__restrict__ F_all, int b, int H, int t, int m,
                                            int lmin, const double (&v)[4]) {
     const size_t rs = (size_t)(p.nrings - 1 - t);
+    if (!JHTB_IN((long long)rs * p.M + m, (long long)p.nrings * p.M, 301)) return;
     if (SPIN) {
         const double ssign = ((m + lmin) & 1) ? -1.0 : 1.0;
         double2 *Fp = F_all + (size_t)b * 2 * p.nrings * p.M;
@@ -548,6 +549,8 @@ __global__ void tc_prep_kernel(int lmax, long long K, const SeedParam *__restric
 }
 
 }  // namespace
+
+JHTB_DEBUG_ACCESSOR(tc_synth)
 
 template <int SPIN, int BM>
 static int launch_tc_synth_t(const Plan &p, const TcParams &q, const double2 *alm, double2 *F, int nb, cudaStream_t s) {

@@ -43,7 +43,7 @@ __global__ void weighted_residual_kernel(const double *__restrict__ maps, const 
                 r = 4LL * nside - 2 - (ii - 1);
             }
             const long long half = r < 2LL * nside ? r : 4LL * nside - 2 - r;
-            w = base * (1.0 + ring_w[half]);
+            w = JHTB_IN(half, 2LL * nside, 501) ? base * (1.0 + ring_w[half]) : 0.0;  // the ring weights of the half grid
         }
         const double v = synth ? maps[i] - synth[i] : maps[i];
         out[i] = w * v;
@@ -91,6 +91,8 @@ int grid_for(long long n) {
 }
 
 }  // namespace
+
+JHTB_DEBUG_ACCESSOR(vecops)
 }  // namespace jhtb
 
 using namespace jhtb;

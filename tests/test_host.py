@@ -155,7 +155,7 @@ def test_real_dof_is_an_isometry(lmax, spin):
     a = masked.real_to_alm(x, lmax, spin)
     back = masked.alm_to_real(a, lmax, spin)
     np.testing.assert_allclose(back.numpy(), x.numpy(), rtol=0, atol=1e-15)
-    G = torch.as_tensor(jhtb.alm_metric_weight(lmax))
+    G = torch.as_tensor(np.array(jhtb.alm_metric_weight(lmax)))
     na = float(torch.sum(G * a.abs() ** 2))
     assert abs(na - float(torch.sum(x * x))) <= 1e-12 * max(1.0, na)
     # batch helpers used by the CG agree with the single-vector form
@@ -273,3 +273,21 @@ def test_tuning_table_lookup(tmp_path):
 
 def test_tuning_knobs_reject_null_plan(lib):
     assert lib.jhtb_plan_set_tuning(None, 1, 256) == _lib.JHTB_ERR_INVALID
+
+
+def test_debug_library_exports_the_same_symbols():
+    """The bounds-checked build (make debug) exports exactly the release library's entry points."""
+    if not _lib.DEBUG_LIB_PATH.exists():
+        pytest.skip("debug library not built")
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.DEBUG_LIB_PATH)], capture_output=True, text=True,
+                         check=True)
+    dyn = {ln.split()[-1] for ln in out.stdout.splitlines() if ln.strip()}
+    assert {s for s in dyn if s.startswith("jhtb_")} == _declared_functions()
+
+
+def test_release_debug_bounds_is_unsupported(lib):
+    cnt, site, idx, ext = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+    rc = lib.jhtb_debug_bounds(ctypes.byref(cnt), ctypes.byref(site), ctypes.byref(idx), ctypes.byref(ext))
+    assert rc == _lib.JHTB_ERR_UNSUPPORTED
+    assert "debug library" in _lib.last_error()
+    assert lib.jhtb_debug_bounds(None, None, None, None) == _lib.JHTB_ERR_INVALID
