@@ -140,7 +140,7 @@ DEBUG_LIB_PATH = LIB_PATH.parent.parent / "_lib_debug" / "libjhtb.so"
 def debug_bounds(lib=None) -> dict:
     """The bounds-check record of a debug library (``make debug``): failed accesses since
     the last call, with the first one's site code, index and extent (clears the record).
-    Raises JhtbError (status JHTB_ERR_UNSUPPORTED) on the release library."""
+    Raises NotImplementedError (status JHTB_ERR_UNSUPPORTED) on the release library."""
     lib = lib or load_library()
     cnt, site, idx, ext = ctypes.c_int64(), ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
     check(lib.jhtb_debug_bounds(ctypes.byref(cnt), ctypes.byref(site), ctypes.byref(idx), ctypes.byref(ext)),

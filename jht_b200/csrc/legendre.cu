@@ -598,14 +598,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj0MinBlocks) adj0_kern
                     double2 prev = make_double2(0.0, 0.0);
                     if (acc && wr && JHTB_IN(b0 + i0 + qw, p.K, 204)) prev = part[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
+                    if (f && q0 + kSub <= cnt) {  // one straight sequence of steps (see adj2_kernel)
 #pragma unroll
-                    for (int q = 0; q < kSub; q += 2) {
-                        if (q0 + q < cnt)
-                            rb.v[q][lane] = f ? adj0_step<R, false>(sb.ag[q0 + q].x, x, u1, u2, sc, UA)
-                                              : adj0_step<R, true>(sb.ag[q0 + q].x, x, u1, u2, sc, UA);
-                        if (q0 + q + 1 < cnt)
-                            rb.v[q + 1][lane] = f ? adj0_step<R, false>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB)
-                                                  : adj0_step<R, true>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB);
+                        for (int q = 0; q < kSub; q += 2) {
+                            rb.v[q][lane] = adj0_step<R, false>(sb.ag[q0 + q].x, x, u1, u2, sc, UA);
+                            rb.v[q + 1][lane] = adj0_step<R, false>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB);
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < kSub; q += 2) {
+                            if (q0 + q < cnt) rb.v[q][lane] = adj0_step<R, true>(sb.ag[q0 + q].x, x, u1, u2, sc, UA);
+                            if (q0 + q + 1 < cnt) rb.v[q + 1][lane] = adj0_step<R, true>(sb.ag[q0 + q + 1].x, x, u1, u2, sc, UB);
+                        }
                     }
                     if (!f) {
                         fast = true;
@@ -746,20 +750,34 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kAdj2MinBlocks) adj2_kern
                     double2 prev = make_double2(0.0, 0.0);
                     if (acc && wr && JHTB_IN(b0 + i0 + qw, p.K, 204)) prev = dstw[b0 + i0 + qw];
                     const bool f = __all_sync(kFull, fast);
+                    // The variant is chosen once per group, not per step: a whole group of
+                    // representable rings runs one straight sequence of steps (choosing per
+                    // step made the two variants' register assignments meet after every step).
+                    if (f && q0 + kSub <= cnt) {
 #pragma unroll
-                    for (int q = 0; q < kSub; q += 2) {
-                        double2 op, om;
-                        if (q0 + q < cnt) {
-                            if (f) adj2_step<R, false, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
-                            else adj2_step<R, true, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                        for (int q = 0; q < kSub; q += 2) {
+                            double2 op, om;
+                            adj2_step<R, false, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
                             rb.v[q][lane] = op;
                             rb.v[kSub + q][lane] = om;
-                        }
-                        if (q0 + q + 1 < cnt) {
-                            if (f) adj2_step<R, false, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
-                            else adj2_step<R, true, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                            adj2_step<R, false, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
                             rb.v[q + 1][lane] = op;
                             rb.v[kSub + q + 1][lane] = om;
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < kSub; q += 2) {
+                            double2 op, om;
+                            if (q0 + q < cnt) {
+                                adj2_step<R, true, 1>(sb.ag[q0 + q].x, sb.ag[q0 + q].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                                rb.v[q][lane] = op;
+                                rb.v[kSub + q][lane] = om;
+                            }
+                            if (q0 + q + 1 < cnt) {
+                                adj2_step<R, true, -1>(sb.ag[q0 + q + 1].x, sb.ag[q0 + q + 1].y, x, p1, p2, sp, m1, m2, sm, in, op, om);
+                                rb.v[q + 1][lane] = op;
+                                rb.v[kSub + q + 1][lane] = om;
+                            }
                         }
                     }
                     if (!f) {

@@ -30,6 +30,10 @@ namespace {
 #endif
 constexpr int kFftThreads = JHTB_FFT_THREADS;  // threads per ring CTA
 constexpr int kFftMinBlocks = JHTB_FFT_MINB;   // resident ring CTAs per SM (4096-point buffers)
+#ifndef JHTB_PIECE_MINB
+#define JHTB_PIECE_MINB 2
+#endif
+constexpr int kPieceMinBlocks = JHTB_PIECE_MINB;  // resident CTAs per SM of the piece kernels
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -264,11 +268,19 @@ __device__ __forceinline__ void stockham_pass_sm(double2 *buf, int n, int Ns, do
 
 // The FFT with every pass inlined (no call boundary, so no register saves to the stack
 // around the passes) and shared-memory twiddles; for kernels that run one or two transforms.
+// Largest radix of the piece kernels' passes (16: fewer passes; 8: fewer registers).
+#ifndef JHTB_PIECE_RADIX
+#define JHTB_PIECE_RADIX 16
+#endif
 __device__ __forceinline__ void fft_stockham_sm(double2 *buf, int n, double dir, const double2 *T) {
     int bits = ilog2i(n), Ns = 1;
-    for (; bits >= 4; bits -= 4, Ns <<= 4) stockham_pass_sm<16>(buf, n, Ns, dir, T);
-    if (bits == 3) stockham_pass_sm<8>(buf, n, Ns, dir, T);
-    else if (bits == 2) stockham_pass_sm<4>(buf, n, Ns, dir, T);
+    if (JHTB_PIECE_RADIX >= 16) {
+        for (; bits >= 4; bits -= 4, Ns <<= 4) stockham_pass_sm<16>(buf, n, Ns, dir, T);
+        if (bits == 3) stockham_pass_sm<8>(buf, n, Ns, dir, T);
+    } else {
+        for (; bits >= 3; bits -= 3, Ns <<= 3) stockham_pass_sm<8>(buf, n, Ns, dir, T);
+    }
+    if (bits == 2) stockham_pass_sm<4>(buf, n, Ns, dir, T);
     else if (bits == 1) stockham_pass_sm<2>(buf, n, Ns, dir, T);
 }
 
@@ -737,7 +749,7 @@ __device__ __forceinline__ double2 fold_one(const double2 *__restrict__ Fp, cons
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_piece_kernel(const int *__restrict__ piece_list,
+__global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_synth_piece_kernel(const int *__restrict__ piece_list,
                                                                            const RingDesc *__restrict__ rings, int lmax,
                                                                            int M, int nrings, long long npix,
                                                                            const double2 *__restrict__ F_all,
@@ -827,7 +839,7 @@ __global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_synth_piece_k
 }
 
 template <int SPIN>
-__global__ void __launch_bounds__(kFftThreads, kFftMinBlocks) ring_adjoint_piece_kernel(const int *__restrict__ piece_list,
+__global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_adjoint_piece_kernel(const int *__restrict__ piece_list,
                                                                              const RingDesc *__restrict__ rings, int lmax,
                                                                              int M, int nrings, long long npix,
                                                                              const double *__restrict__ maps_all,

@@ -146,7 +146,7 @@ __device__ __forceinline__ double tc_step(double t, double &u1, double &u2, int 
     return (SLOW && sc != 0) ? 0.0 : u;
 }
 
-// 16 steps of this thread's CH recursion chains (GEMMs J0 .. J0 + CH - 1), split into
+// 16 steps of this thread's CH recursion chains (GEMMs j0 .. j0 + CH - 1), split into
 // BF16 parts and stored as its row (= its tensor-memory lane) of those GEMMs' three A
 // operands: tA[c] is the lane-offset tensor-memory address of chain c's split-0 operand,
 // the splits following at ACOLS columns apart.  Spin 2: GEMM 0 is the +2 recursion
@@ -158,9 +158,10 @@ __device__ __forceinline__ double tc_step(double t, double &u1, double &u2, int 
 // leave the state untouched.  Each half-chunk first loads its eight coefficient pairs
 // and forms the multipliers t = alpha x +- gamma, so only one FMA per step stays on the
 // dependency chain.
-template <bool SLOW, bool FIRST, int CH, int J0>
+template <bool SLOW, bool FIRST, int CH>
 __device__ __forceinline__ void tc_chunk(const double2 *coef, const double (&x)[CH], double (&u1)[CH],
-                                         double (&u2)[CH], int (&sc)[CH], const uint32_t (&tA)[CH], int skip) {
+                                         double (&u2)[CH], int (&sc)[CH], const uint32_t (&tA)[CH], int skip,
+                                         unsigned long long gflip) {
     constexpr uint32_t AC = kTcK / 2;
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
@@ -169,7 +170,12 @@ __device__ __forceinline__ void tc_chunk(const double2 *coef, const double (&x)[
         for (int k = 0; k < 8; ++k) {
             const double2 a = coef[half * 8 + k];
 #pragma unroll
-            for (int c = 0; c < CH; ++c) t[c][k] = ((J0 + c) & 1) ? fma(a.x, x[c], -a.y) : fma(a.x, x[c], a.y);
+            for (int c = 0; c < CH; ++c) {
+                // GEMM j0 + c runs the +gamma recursion when j0 + c is even, -gamma when odd:
+                // gflip holds the sign bit of chain c (bit 63 - c), applied as an exact flip
+                const double g = __longlong_as_double(__double_as_longlong(a.y) ^ (long long)((gflip << c) & (1ull << 63)));
+                t[c][k] = fma(a.x, x[c], g);
+            }
         }
         uint32_t pk[CH][3][4];
         double v[CH][8];
@@ -210,12 +216,13 @@ __device__ __forceinline__ void tc_store_F(const TcParams &p, double2 *__restric
     }
 }
 
-// acc[col + e][row] (+)= the 8 FP32 block sums at tensor-memory address ta.
-__device__ __forceinline__ void fold8(double *accj, uint32_t ta, int col, int row, bool first) {
-    float v[8];
-    tmem_ld8(ta, v);
+// acc[col + e][row] (+)= the 32 FP32 block sums at tensor-memory address ta: one tensor-
+// memory load and wait for the 32 columns, then their 32 shared-memory sums.
+__device__ __forceinline__ void fold32(double *accj, uint32_t ta, int col, int row, bool first) {
+    float v[32];
+    tmem_ld32(ta, v);
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
+    for (int e = 0; e < 32; ++e) {
         double *a = accj + (size_t)(col + e) * kTcRows + row;
         *a = first ? (double)v[e] : *a + (double)v[e];
     }
@@ -232,6 +239,12 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
     constexpr int CH = C::CH;
     const int row = (warp & 3) * 32 + lane;  // A row = TMEM lane (warp w reaches lanes 32 (w % 4) ..)
     const int j0 = (warp >> 2) * CH;         // this thread's first GEMM
+    // sign bits of gamma for the thread's chains: chain c (GEMM j0 + c) is the -gamma
+    // recursion when j0 + c is odd; bit 63 - c of gflip (spin 0 has gamma = 0)
+    unsigned long long gflip = 0;
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+        if ((j0 + c) & 1) gflip |= 1ull << (63 - c);
     const uint32_t tl = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     const int nitems = p.norder;
     unsigned gc = 0, bk = 0;
@@ -267,16 +280,12 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
             for (int e = 0; e < CH; ++e) tA[e] = tl + (uint32_t)(C::COL_A + (sA * C::NG + j0 + e) * 3 * C::ACOLS);
             const double2 *coef = reinterpret_cast<const double2 *>(sm.B[sB] + C::NBT * 3 * C::BTILE);
             const bool f = __all_sync(0xffffffffu, fast);
-            if (c == 0) {  // the first chunk: steps before the start state are dead
-                if (j0 == 0) tc_chunk<true, true, CH, 0>(coef, x, u1, u2, sc, tA, q.skip);
-                else tc_chunk<true, true, CH, 1>(coef, x, u1, u2, sc, tA, q.skip);
-            } else if (j0 == 0) {
-                if (f) tc_chunk<false, false, CH, 0>(coef, x, u1, u2, sc, tA, 0);
-                else tc_chunk<true, false, CH, 0>(coef, x, u1, u2, sc, tA, 0);
-            } else {
-                if (f) tc_chunk<false, false, CH, 1>(coef, x, u1, u2, sc, tA, 0);
-                else tc_chunk<true, false, CH, 1>(coef, x, u1, u2, sc, tA, 0);
-            }
+            if (c == 0)  // the first chunk: steps before the start state are dead
+                tc_chunk<true, true, CH>(coef, x, u1, u2, sc, tA, q.skip, gflip);
+            else if (f)
+                tc_chunk<false, false, CH>(coef, x, u1, u2, sc, tA, 0, gflip);
+            else
+                tc_chunk<true, false, CH>(coef, x, u1, u2, sc, tA, 0, gflip);
             if (!f || c == 0) {
                 fast = true;
 #pragma unroll
@@ -301,11 +310,11 @@ __device__ void tc_producer(const TcParams &p, TcSmem<SPIN, BM> &sm, double2 *__
                     double *accj = &sm.acc[j][0][0];
                     const uint32_t th = tl + (uint32_t)((kb * C::NG + j) * N);
 #pragma unroll 1
-                    for (int col = 0; col < N; col += 8) fold8(accj, th + col, col, row, first_block);
+                    for (int col = 0; col < N; col += 32) fold32(accj, th + col, col, row, first_block);
                     if (last) {
                         const uint32_t tcorr = tl + (uint32_t)(C::COL_CORR + j * N);
 #pragma unroll 1
-                        for (int col = 0; col < N; col += 8) fold8(accj, tcorr + col, col, row, false);
+                        for (int col = 0; col < N; col += 32) fold32(accj, tcorr + col, col, row, false);
                     }
                 }
                 tc_fence_before();
