@@ -10,11 +10,15 @@ each stage launch inside the C ABI (jhtb_plan_set_timing); the FP64 roofline
 denominator is measured with the in-library FMA probe.
 
 ``mixed`` is the batched mixed-precision form of the same step: B maps per step,
-the synthesis on the tensor cores (split-BF16 products, FP32 accumulation folded
-into FP64), the VJP's adjoint and the ring transforms in FP64; it reports maps/s,
-the ratio to the FP64 maps/s, and the relative error of every map and gradient
-against the FP64 path on the same inputs.
+both Legendre stages (the synthesis and the VJP's adjoint) on the tensor cores
+(split-BF16 products, FP32 accumulation folded into FP64), the recursion, the ring
+transforms and the loss in FP64; it reports maps/s, the ratio to the FP64 maps/s, and
+the relative error of every map and gradient against the FP64 path on the same inputs.
 
+``configs`` (secondary lines): spin-0 analysis(niter=3) at nside 1024 / lmax 2048 (FP64
+and tensor-core A0 with FP64 residuals, error vs FP64), 64 spin-0 maps S + S^T at
+nside 512 / lmax 1024 (FP64 and bf16x3, per-map error), and the 16-RHS masked CG at
+nside 512 / lmax 1024 (ms per iteration for both operator precisions).
 ``offgrid`` (secondary) times the off-grid synthesis_general and its adjoint at lmax 2048 on
 10^7 seeded points.
 
@@ -56,7 +60,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--nside", type=int, default=2048)
     ap.add_argument("--lmax", type=int, default=4096)
-    ap.add_argument("--cpu-sample-m", type=int, default=64,
+    ap.add_argument("--cpu-sample-m", type=int, default=96,
                     help="orders in the CPU-baseline sample (the same sample for cpu_baseline and --impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mixed-batch", type=int, default=16, help="maps per step of the mixed-precision form (0: skip)")
@@ -654,7 +658,7 @@ def main():
         if mt:
             traffic = float(mt.group(1))
 
-    # ---- batched mixed precision: tensor-core synthesis, FP64 adjoint ------------------
+    # ---- batched mixed precision: both Legendre stages on the tensor cores ------------------
     mixed = None
     if args.mixed_batch > 0:
         mixed = run_mixed(args, jhtb, _lib, torch, dev, pg, nside, lmax, spin, rank, world, ms_per_step)

@@ -34,6 +34,10 @@ constexpr int kFftMinBlocks = JHTB_FFT_MINB;   // resident ring CTAs per SM (409
 #define JHTB_PIECE_MINB 2
 #endif
 constexpr int kPieceMinBlocks = JHTB_PIECE_MINB;  // resident CTAs per SM of the piece kernels
+#ifndef JHTB_PIECE_U
+#define JHTB_PIECE_U 4
+#endif
+constexpr int kUP = JHTB_PIECE_U;  // elements per thread whose gathers the piece kernels issue together
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -772,23 +776,23 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_synth_piece
     double *outQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     double *outU = outQ + npix;
     const int bd = blockDim.x;
-    // a_s[k1]: the Q aliases k1 + Lq k2 of the phased fold, kU values of k1 per thread at a time
-    for (int k10 = threadIdx.x; k10 < Lq; k10 += kU * bd) {
-        double2 acc[kU];
+    // a_s[k1]: the Q aliases k1 + Lq k2 of the phased fold, kUP values of k1 per thread at a time
+    for (int k10 = threadIdx.x; k10 < Lq; k10 += kUP * bd) {
+        double2 acc[kUP];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) acc[u] = make_double2(0.0, 0.0);
-        // every load of the kU x Q terms (and, for a power of two, of the kU twiddles) is
+        for (int u = 0; u < kUP; ++u) acc[u] = make_double2(0.0, 0.0);
+        // every load of the kUP x Q terms (and, for a power of two, of the kUP twiddles) is
         // issued before the first is used
-        double2 d[kMaxPieces][kU], w1[kU];
+        double2 d[kMaxPieces][kUP], w1[kUP];
 #pragma unroll
         for (int k2 = 0; k2 < kMaxPieces; ++k2)
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < kUP; ++u) {
                 const int k1 = k10 + u * bd;
                 d[k2][u] = (k2 < Q && k1 < Lq) ? fold_one(Fp, Fm, k1 + Lq * k2, N, lmax, shifted) : make_double2(0.0, 0.0);
             }
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUP; ++u) {
             const int k1 = k10 + u * bd;
             w1[u] = (!split && k1 < Lq) ? tw_pi(tw, (long long)c * k1, N) : make_double2(1.0, 0.0);
         }
@@ -799,10 +803,10 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_synth_piece
             if (k2 >= Q) break;
             const double2 w = root8((4 / Q) * c * k2);
 #pragma unroll
-            for (int u = 0; u < kU; ++u) acc[u] = cadd(acc[u], k2 ? cmul(d[k2][u], w) : d[k2][u]);
+            for (int u = 0; u < kUP; ++u) acc[u] = cadd(acc[u], k2 ? cmul(d[k2][u], w) : d[k2][u]);
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUP; ++u) {
             const int k1 = k10 + u * bd;
             if (k1 >= Lq) continue;
             // power of two: e^{i pi c k1 / N} from the table; kSplit4: e^{i pi c k1 / N} times the
@@ -817,12 +821,12 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_synth_piece
     __syncthreads();
     if (split) {  // E[j] = w(j) sum_k (a[k] w(k)) conj(w(j - k)): FFT, chirp spectrum, inverse FFT
         fft_stockham_sm(buf, L, -1.0, T);
-        for (int q0 = threadIdx.x; q0 < L; q0 += kU * bd) {
-            double2 w[kU];
+        for (int q0 = threadIdx.x; q0 < L; q0 += kUP * bd) {
+            double2 w[kUP];
 #pragma unroll
-            for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < L ? bh_get(bh + rd.bh_off, L, q0 + u * bd, 1) : make_double2(0.0, 0.0);
+            for (int u = 0; u < kUP; ++u) w[u] = q0 + u * bd < L ? bh_get(bh + rd.bh_off, L, q0 + u * bd, 1) : make_double2(0.0, 0.0);
 #pragma unroll
-            for (int u = 0; u < kU; ++u)
+            for (int u = 0; u < kUP; ++u)
                 if (q0 + u * bd < L) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
         }
         __syncthreads();
@@ -862,21 +866,21 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_adjoint_pie
     double2 *Vm = SPIN ? Vp + (size_t)nrings * M : Vp;
     const int bd = blockDim.x;
     // b_s[j1]: the Q pixels j1 + Lq j2 with e^{-2 pi i s j / N}
-    for (int j10 = threadIdx.x; j10 < Lq; j10 += kU * bd) {
-        double2 acc[kU];
+    for (int j10 = threadIdx.x; j10 < Lq; j10 += kUP * bd) {
+        double2 acc[kUP];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) acc[u] = make_double2(0.0, 0.0);
-        double2 a[kMaxPieces][kU], w1[kU];  // every load issued before the first is used
+        for (int u = 0; u < kUP; ++u) acc[u] = make_double2(0.0, 0.0);
+        double2 a[kMaxPieces][kUP], w1[kUP];  // every load issued before the first is used
 #pragma unroll
         for (int j2 = 0; j2 < kMaxPieces; ++j2)
 #pragma unroll
-            for (int u = 0; u < kU; ++u) {
+            for (int u = 0; u < kUP; ++u) {
                 const int j = j10 + u * bd + Lq * j2;
                 a[j2][u] = (j2 < Q && j10 + u * bd < Lq && JHTB_IN(rd.start + j, npix, 103)) ? make_double2(inQ[j], SPIN ? inU[j] : 0.0)
                                                                                             : make_double2(0.0, 0.0);
             }
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUP; ++u) {
             const int j1 = j10 + u * bd;
             w1[u] = (!split && j1 < Lq) ? tw_pi(tw, -2LL * s * j1, N) : make_double2(1.0, 0.0);
         }
@@ -887,10 +891,10 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_adjoint_pie
             if (j2 >= Q) break;
             const double2 w = root8(-(8 / Q) * s * j2);
 #pragma unroll
-            for (int u = 0; u < kU; ++u) acc[u] = cadd(acc[u], j2 ? cmul(a[j2][u], w) : a[j2][u]);
+            for (int u = 0; u < kUP; ++u) acc[u] = cadd(acc[u], j2 ? cmul(a[j2][u], w) : a[j2][u]);
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUP; ++u) {
             const int j1 = j10 + u * bd;
             if (j1 >= Lq) continue;
             // power of two: e^{-2 pi i s j1 / N} from the table; kSplit4: times the chirp
@@ -905,12 +909,12 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_adjoint_pie
     __syncthreads();
     fft_stockham_sm(buf, L, -1.0, T);
     if (split) {  // W[k] = conj(w(k)) sum_j (b[j] conj(w(j))) w(k - j)
-        for (int q0 = threadIdx.x; q0 < L; q0 += kU * bd) {
-            double2 w[kU];
+        for (int q0 = threadIdx.x; q0 < L; q0 += kUP * bd) {
+            double2 w[kUP];
 #pragma unroll
-            for (int u = 0; u < kU; ++u) w[u] = q0 + u * bd < L ? bh_get(bh + rd.bh_off, L, q0 + u * bd, -1) : make_double2(0.0, 0.0);
+            for (int u = 0; u < kUP; ++u) w[u] = q0 + u * bd < L ? bh_get(bh + rd.bh_off, L, q0 + u * bd, -1) : make_double2(0.0, 0.0);
 #pragma unroll
-            for (int u = 0; u < kU; ++u)
+            for (int u = 0; u < kUP; ++u)
                 if (q0 + u * bd < L) buf[pidx(q0 + u * bd)] = cmul(buf[pidx(q0 + u * bd)], w[u]);
         }
         __syncthreads();
@@ -922,9 +926,9 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_adjoint_pie
     // V rows: Vp[m] = W[m mod N] for m = s (mod Q), Vm[m] = conj(W[-m mod N]) for m = -s (mod Q),
     // both times e^{-i m phi0} (gather_adjoint, restricted to this piece's residue class)
     const int sm = (Q - s) % Q;
-    for (int m0 = threadIdx.x * Q; m0 <= lmax; m0 += kU * bd * Q) {
+    for (int m0 = threadIdx.x * Q; m0 <= lmax; m0 += kUP * bd * Q) {
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUP; ++u) {
             const int mp = m0 + u * bd * Q + s;  // Vp orders
             if (mp <= lmax) {
                 const int kp = (mp % N - s) / Q;
