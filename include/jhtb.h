@@ -255,6 +255,18 @@ int jhtb_plan_set_tuning(jhtb_plan *plan, int key, int value);
 #define JHTB_FAULT_STALL 1
 int jhtb_plan_inject_fault(jhtb_plan *plan, int kind);
 
+/* Batched complex FP64 FFT of a 2,3,5-smooth length n <= 10240 (replaces the jnp.fft calls of
+ * jht's off-grid transforms, _nufft.py:164-191; longer transforms are composed by the caller
+ * from two calls, four-step).  Transform b = o * inner + t (o < howmany / inner, t < inner)
+ * reads x[i] = in[o * in_dist_outer + t * in_dist_inner + i * in_stride] (complex128
+ * elements) and writes out[o * out_dist_outer + t * out_dist_inner + k * out_stride] =
+ * scale * w_k * sum_i x[i] e^{sign 2 pi i i k / n}, with w_k = e^{sign 2 pi i (t k mod
+ * twiddle_n) / twiddle_n} when twiddle_n > 0 (the four-step twiddle), else 1.  sign = -1
+ * (forward) or +1.  In place (out == in) only with the same input and output layout. */
+int jhtb_fft_c2c(const void *in, void *out, int n, int64_t howmany, int64_t inner, int64_t in_stride,
+                 int64_t in_dist_outer, int64_t in_dist_inner, int64_t out_stride, int64_t out_dist_outer,
+                 int64_t out_dist_inner, int sign, double scale, int64_t twiddle_n, void *stream);
+
 /* Bounds-check record of a debug library (no counterpart in jht; the replacement for a
  * memory checker on machines where none can run).  A library built with `make debug`
  * (jht_b200/_lib_debug/libjhtb.so, -DJHTB_DEBUG) tests every checked gather and scatter

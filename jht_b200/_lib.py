@@ -56,6 +56,7 @@ EXPORTS = (
     "jhtb_nufft_spread",
     "jhtb_nufft_spread_tiles",
     "jhtb_debug_bounds",
+    "jhtb_fft_c2c",
 )
 
 
@@ -124,6 +125,8 @@ def load_library(path: str | os.PathLike | None = None):
                                               vp, vp]),
             "jhtb_debug_bounds": (i32, [ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i64),
                                         ctypes.POINTER(i64)]),
+            "jhtb_fft_c2c": (i32, [vp, vp, i32, i64, i64, i64, i64, i64, i64, i64, i64, i32, ctypes.c_double, i64,
+                                   vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)

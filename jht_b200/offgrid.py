@@ -10,8 +10,9 @@ matches ducc's ``sphere_interpol``), mapped onto the device:
    kernels on a ring-set plan (``jhtb_plan_create_rings`` + ``jhtb_legendre_synthesis``);
 2. the double-Fourier-sphere extension to the 2 pi theta period and a theta FFT
    (offgrid.py:113-129), then the deconvolution by the kernel's Fourier transform and an
-   inverse 2D FFT onto the oversampled torus grid (_nufft.py:164-174) -- gathers and
-   cuFFT through torch;
+   inverse 2D FFT onto the oversampled torus grid (_nufft.py:164-174) -- gathers and the
+   library's FFT kernel (``jhtb_fft_c2c``, 2,3,5-smooth lengths; the 2-D transform skips
+   the grid's all-zero rows);
 3. the W x W exponential-of-semicircle window sums at the points
    (``jhtb_nufft_interp``, _nufft.py:150-178).
 
@@ -34,6 +35,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import _fft
 from .healpix import _adjoint_cotangent_input, _as_alm, _device, _synthesis_cotangent, alm_metric_weight, alm_size
 
 __all__ = ["synthesis_general", "adjoint_synthesis_general"]
@@ -170,10 +172,15 @@ def _torus_grid(g: _Geometry, F: torch.Tensor) -> torch.Tensor:
     cols[:ns, L:] = Fp
     cols[:ns, :L] = torch.conj(torch.flip(Fm[:, 1:], dims=(1,)))
     cols[g.south] = g.sign_m[None, :] * cols[g.refl]
-    Fk = torch.fft.fftshift(torch.fft.fft(cols, dim=0, norm="forward"), dim=0)
+    # theta FFT (1/nd scaled, as norm="forward"), centred: the shift of an even length is a roll
+    Fk = torch.roll(_fft.fft(cols, 0, -1, 1.0 / nd), nd // 2, dims=0)
+    # the unscaled inverse 2-D FFT of the zero-padded grid: rows first, only the nd non-zero
+    # rows (the other rows stay zero), then every column
+    Crow = torch.zeros((nd, g.nm), dtype=torch.complex128, device=F.device)
+    Crow[:, g.mpos] = Fk * g.inv_corr
     C = torch.zeros((g.nk, g.nm), dtype=torch.complex128, device=F.device)
-    C[g.kpos[:, None], g.mpos[None, :]] = Fk * g.inv_corr
-    return torch.fft.ifft2(C, norm="forward")
+    C[g.kpos] = _fft.fft(Crow, 1, +1)
+    return _fft.fft(C, 0, +1)
 
 
 def _interp(g: _Geometry, grid: torch.Tensor, theta: torch.Tensor, phi: torch.Tensor, deriv: bool):
@@ -236,8 +243,10 @@ def _adjoint(g: _Geometry, fc: torch.Tensor, theta: torch.Tensor, phi: torch.Ten
         st = g.plan.lib.jhtb_nufft_spread(fc.contiguous().data_ptr(), theta.data_ptr(), phi.data_ptr(), theta.numel(),
                                           g.nk, g.nm, g.W, ctypes.c_double(g.beta), grid.data_ptr(), _stream())
         _lib.check(st, "jhtb_nufft_spread")
-    G = torch.fft.fft2(grid)[g.kpos[:, None], g.mpos[None, :]] * g.inv_corr
-    d = torch.fft.ifft(torch.fft.ifftshift(G, dim=0), dim=0)
+    # the forward 2-D FFT restricted to the nd x Nm centred modes: every column, then the
+    # nd rows that are kept; then the scaled inverse theta FFT of the uncentred columns
+    G = _fft.fft(_fft.fft(grid, 0, -1)[g.kpos], 1, -1)[:, g.mpos] * g.inv_corr
+    d = _fft.fft(torch.roll(G, -(nd // 2), dims=0), 0, +1, 1.0 / nd)
     top = d[:ns].clone()
     top.index_add_(0, g.refl, g.sign_m[None, :] * d[g.south])
     V = torch.zeros((g.ncomp, ns, L + 1), dtype=torch.complex128, device=fc.device)

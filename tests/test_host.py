@@ -291,3 +291,21 @@ def test_release_debug_bounds_is_unsupported(lib):
     assert rc == _lib.JHTB_ERR_UNSUPPORTED
     assert "debug library" in _lib.last_error()
     assert lib.jhtb_debug_bounds(None, None, None, None) == _lib.JHTB_ERR_INVALID
+
+
+def test_fft_split_and_argument_checks(lib):
+    """The four-step split of the off-grid FFT lengths, and the C entry point's argument
+    checks (made before any device work)."""
+    from jht_b200 import _fft
+
+    for n in (12288, 17280, 30000, 34560, 102400):
+        n1, n2 = _fft._split(n)
+        assert n1 * n2 == n and n1 <= _fft.SM_MAX and n2 <= _fft.SM_MAX
+        assert _fft._smooth(n1) and _fft._smooth(n2)
+    buf = ctypes.c_void_p(16)
+    args = (1, 1, 1, 1, 0, 1, 1, 0, -1, 1.0, 0, None)
+    assert lib.jhtb_fft_c2c(buf, buf, 7, *args) == _lib.JHTB_ERR_INVALID      # not 2,3,5-smooth
+    assert "smooth" in _lib.last_error()
+    assert lib.jhtb_fft_c2c(buf, buf, 20480, *args) == _lib.JHTB_ERR_INVALID  # above the shared-memory limit
+    assert lib.jhtb_fft_c2c(buf, buf, 8, 1, 1, 1, 1, 0, 1, 1, 0, 2, 1.0, 0, None) == _lib.JHTB_ERR_INVALID  # sign
+    assert lib.jhtb_fft_c2c(None, buf, 8, *args) == _lib.JHTB_ERR_INVALID
