@@ -4,7 +4,8 @@ Every checked gather and scatter index of its kernels is tested against the exte
 its buffer; an access out of range is skipped and counted (jhtb_debug_bounds).  A child
 process loads the debug library (JHTB_LIBRARY), runs the transforms over geometries that
 reach every code path of the azimuthal stage (whole rings, power-of-two pieces of the
-belt, chirp-z pieces of the polar caps, aliasing short rings) and of the Legendre kernels
+belt, chirp-z pieces of the polar caps, chirp-z rings split through the scratch rows at
+nside 4096, aliasing short rings) and of the Legendre kernels
 (FP64 and tensor-core, spin 0 and 2, full and partial map groups), and must record no
 failed access; its outputs must equal the release library's on the same inputs.
 """
@@ -36,7 +37,8 @@ ROOT = Path(__file__).resolve().parents[1]
 CASES = [
     (1, 4, 0, 1, "fp64"), (2, 5, 2, 1, "fp64"), (12, 20, 2, 1, "fp64"), (16, 40, 0, 1, "fp64"),
     (64, 128, 0, 1, "fp64"), (512, 1024, 2, 1, "fp64"), (1024, 2048, 0, 1, "fp64"),
-    (2048, 4096, 2, 1, "fp64"), (64, 128, 2, 3, "bf16x3"), (256, 512, 0, 17, "bf16x3"),
+    (2048, 4096, 2, 1, "fp64"), (4096, 96, 2, 1, "fp64"), (4096, 96, 0, 1, "fp64"), (64, 128, 2, 3, "bf16x3"),
+    (256, 512, 0, 17, "bf16x3"),
 ]
 
 CHILD = textwrap.dedent("""
