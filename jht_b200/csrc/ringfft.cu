@@ -218,13 +218,17 @@ __device__ __forceinline__ void fft_stockham(double2 *buf, int n, double dir, co
 // Twiddles from shared memory: e^{-2 pi i x / kFftPiece} = T[x >> 6] T[64 + (x & 63)] with
 // T[a] = e^{-2 pi i a / 64} and T[64 + b] = e^{-2 pi i b / kFftPiece} (each entry rounded once,
 // the product adds about one rounding), so the passes make no global loads.
-constexpr int kSmTwLen = 128;
+// Eight more entries T[128 + g] = e^{-2 pi i g / kTwLen} refine it to kTwLen points (the ring
+// phases and piece twiddles of power-of-two rings up to kTwLen / 2 points).
+constexpr int kSmTwLen = 136;
+constexpr int kSmTwFine = kTwLen / kFftPiece;  // 8
 static_assert(kFftPiece == 64 * 64, "two-level twiddle table of kFftPiece points");
 __device__ __forceinline__ void sm_tw_init(double2 *T) {
     for (int a = threadIdx.x; a < kSmTwLen; a += blockDim.x) {
         double s, c;
         if (a < 64) sincospi(-2.0 * (double)a / 64.0, &s, &c);
-        else sincospi(-2.0 * (double)(a - 64) / (double)kFftPiece, &s, &c);
+        else if (a < 128) sincospi(-2.0 * (double)(a - 64) / (double)kFftPiece, &s, &c);
+        else sincospi(-2.0 * (double)(a - 128) / (double)kTwLen, &s, &c);
         T[a] = make_double2(c, s);
     }
 }
@@ -232,6 +236,16 @@ __device__ __forceinline__ double2 sm_tw(const double2 *T, int x, bool plus) {  
     x &= kFftPiece - 1;
     double2 w = cmul(T[x >> 6], T[64 + (x & 63)]);
     if (plus) w.y = -w.y;
+    return w;
+}
+
+// e^{+i pi a / N} for a power-of-two N, kFftPiece / 2 <= N <= kTwLen / 2, from the shared
+// table: with x = a mod 2N = q y + f (q = 2N / kFftPiece), the conjugate of
+// e^{-2 pi i y / kFftPiece} e^{-2 pi i f / 2N}.
+__device__ __forceinline__ double2 sm_tw_pi(const double2 *T, long long a, int N) {
+    const int x = (int)(a & (2LL * N - 1)), q = 2 * N / kFftPiece;
+    double2 w = cmul(sm_tw(T, x / q, false), T[128 + (x % q) * (kSmTwFine / q)]);
+    w.y = -w.y;
     return w;
 }
 
@@ -776,8 +790,30 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_synth_piece
     double *outQ = maps_all + (size_t)blockIdx.y * nchan * npix + rd.start;
     double *outU = outQ + npix;
     const int bd = blockDim.x;
+    if (!split && Q == 2) {
+        // the belt's two-piece rings: 2 kUP values of k1 per thread and round (two loads each,
+        // all issued first), twiddles from the shared table
+        constexpr int U = 2 * kUP;
+        const double2 r1 = root8(2 * c);  // e^{i pi c / 2}: exactly +-1 or +-i
+        for (int k10 = threadIdx.x; k10 < Lq; k10 += U * bd) {
+            double2 d0[U], d1[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k1 = k10 + u * bd;
+                d0[u] = k1 < Lq ? fold_one(Fp, Fm, k1, N, lmax, shifted) : make_double2(0.0, 0.0);
+                d1[u] = k1 < Lq ? fold_one(Fp, Fm, k1 + Lq, N, lmax, shifted) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k1 = k10 + u * bd;
+                if (k1 >= Lq) continue;
+                const double2 v = cmul(cadd(d0[u], cmul(d1[u], r1)), sm_tw_pi(T, (long long)c * k1, N));
+                if (JHTB_IN(pidx(k1), kFftBufLen, 106)) buf[pidx(k1)] = v;
+            }
+        }
+    }
     // a_s[k1]: the Q aliases k1 + Lq k2 of the phased fold, kUP values of k1 per thread at a time
-    for (int k10 = threadIdx.x; k10 < Lq; k10 += kUP * bd) {
+    for (int k10 = threadIdx.x; k10 < Lq && (split || Q != 2); k10 += kUP * bd) {
         double2 acc[kUP];
 #pragma unroll
         for (int u = 0; u < kUP; ++u) acc[u] = make_double2(0.0, 0.0);
@@ -865,8 +901,32 @@ __global__ void __launch_bounds__(kFftThreads, kPieceMinBlocks) ring_adjoint_pie
     double2 *Vp = V_all + ((size_t)blockIdx.y * nchan * nrings + r) * M;
     double2 *Vm = SPIN ? Vp + (size_t)nrings * M : Vp;
     const int bd = blockDim.x;
+    if (!split && Q == 2) {
+        // the belt's two-piece rings: 2 kUP values of j1 per thread and round (all loads first),
+        // twiddles from the shared table
+        constexpr int U = 2 * kUP;
+        const double sg = (s & 1) ? -1.0 : 1.0;  // e^{-2 pi i s j2 / 2} = (-1)^(s j2)
+        for (int j10 = threadIdx.x; j10 < Lq; j10 += U * bd) {
+            double2 a0[U], a1[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = j10 + u * bd;
+                const bool ok = j < Lq && JHTB_IN(rd.start + j + Lq, npix, 103);
+                a0[u] = ok ? make_double2(inQ[j], SPIN ? inU[j] : 0.0) : make_double2(0.0, 0.0);
+                a1[u] = ok ? make_double2(inQ[j + Lq], SPIN ? inU[j + Lq] : 0.0) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j1 = j10 + u * bd;
+                if (j1 >= Lq) continue;
+                const double2 v = cmul(make_double2(fma(sg, a1[u].x, a0[u].x), fma(sg, a1[u].y, a0[u].y)),
+                                       sm_tw_pi(T, -2LL * s * j1, N));
+                if (JHTB_IN(pidx(j1), kFftBufLen, 106)) buf[pidx(j1)] = v;
+            }
+        }
+    }
     // b_s[j1]: the Q pixels j1 + Lq j2 with e^{-2 pi i s j / N}
-    for (int j10 = threadIdx.x; j10 < Lq; j10 += kUP * bd) {
+    for (int j10 = threadIdx.x; j10 < Lq && (split || Q != 2); j10 += kUP * bd) {
         double2 acc[kUP];
 #pragma unroll
         for (int u = 0; u < kUP; ++u) acc[u] = make_double2(0.0, 0.0);
