@@ -309,3 +309,60 @@ def test_fft_split_and_argument_checks(lib):
     assert lib.jhtb_fft_c2c(buf, buf, 20480, *args) == _lib.JHTB_ERR_INVALID  # above the shared-memory limit
     assert lib.jhtb_fft_c2c(buf, buf, 8, 1, 1, 1, 1, 0, 1, 1, 0, 2, 1.0, 0, None) == _lib.JHTB_ERR_INVALID  # sign
     assert lib.jhtb_fft_c2c(None, buf, 8, *args) == _lib.JHTB_ERR_INVALID
+
+
+def test_fft_four_step_composition_on_a_model_of_the_kernel(monkeypatch):
+    """The host's four-step composition (strides, batch split, twiddle) run against a NumPy
+    model of jhtb_fft_c2c's contract, for lengths above the shared-memory limit."""
+    from jht_b200 import _fft
+
+    mem = {}
+
+    def model(x, out, n, howmany, inner, in_stride, in_do, in_di, out_stride, out_do, out_di, sign, scale, tw):
+        src, dst = mem[x.data_ptr()], mem[out.data_ptr()]
+        i = np.arange(n)
+        for b in range(howmany):
+            o, t = divmod(b, inner)
+            v = src[o * in_do + t * in_di + i * in_stride]
+            y = (np.fft.fft(v) if sign < 0 else np.fft.ifft(v) * n) * scale
+            if tw:
+                y = y * np.exp(sign * 2j * np.pi * ((t * i) % tw) / tw)
+            dst[o * out_do + t * out_di + i * out_stride] = y
+
+    class Buf:
+        def __init__(self, arr):
+            self.arr = arr.reshape(-1)
+            mem[id(self)] = self.arr
+
+        def data_ptr(self):
+            return id(self)
+
+    class T:  # a stand-in for a 2-D complex128 CUDA tensor
+        def __init__(self, a):
+            self.a = np.ascontiguousarray(a)
+            self.buf = Buf(self.a)
+            self.shape = a.shape
+            self.dtype, self.is_cuda = torch.complex128, True
+
+        def dim(self):
+            return 2
+
+        def contiguous(self):
+            return self
+
+        def numel(self):
+            return self.a.size
+
+        def data_ptr(self):
+            return self.buf.data_ptr()
+
+    monkeypatch.setattr(_fft, "_call", model)
+    monkeypatch.setattr(_fft.torch, "empty_like", lambda x: T(np.zeros_like(x.a)))
+    rng = np.random.default_rng(3)
+    for n, other, dim in ((12288, 2, 0), (12288, 3, 1), (17280, 2, 1)):
+        shape = (n, other) if dim == 0 else (other, n)
+        x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        for sign in (-1, 1):
+            got = _fft.fft(T(x), dim, sign, 0.5).a
+            ref = (np.fft.fft(x, axis=dim) if sign < 0 else np.fft.ifft(x, axis=dim) * n) * 0.5
+            assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-12, (n, dim, sign)
