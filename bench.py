@@ -360,7 +360,22 @@ def run_configs(jhtb, _lib, torch, dev) -> dict:
     eb = torch.amax(torch.abs(bmx - b64), dim=1) / torch.amax(torch.abs(b64), dim=1)
     work = 2 * 8.0 * K * 2 * nside * B  # S and S^T, spin 0: 8 flops per triple and map
     pk = _peaks()
+    # the same S + S^T pair through the C ABI on the tuned plan, replayed from a captured CUDA
+    # graph (the autotuner's timing; eager if capture fails)
+    graph_ms, graphed = None, False
+    try:
+        from jht_b200 import autotune
+
+        gplan = _lib.get_plan(nside, lmax, 0, "bf16x3", B)
+        m_out = torch.empty((B, 1, 12 * nside * nside), dtype=torch.float64, device=dev)
+        b_out = torch.empty((B, 1, K), dtype=torch.complex128, device=dev)
+        graph_ms, graphed = autotune._time(gplan, at.reshape(B, 1, K).contiguous(), mmx.reshape(B, 1, -1).contiguous(),
+                                           m_out, b_out, 3)
+        del m_out, b_out
+    except Exception as e:  # noqa: BLE001 - a secondary figure; the line keeps its eager timing
+        graph_ms = f"unavailable: {type(e).__name__}"
     out["batch64_n512_l1024"] = {
+        "mixed_graph_ms": graph_ms, "mixed_graph_captured": graphed,
         "workload": "64 spin-0 maps, synthesis + adjoint, nside 512, lmax 1024, amplitudes log-uniform 1e-2..1e2",
         "fp64_ms": t64, "mixed_ms": tmx, "fp64_maps_per_s": B * 1e3 / t64, "mixed_maps_per_s": B * 1e3 / tmx,
         "mixed_vs_fp64": t64 / tmx,
