@@ -1,20 +1,21 @@
 // Azimuthal stage: per-ring phase shift, m -> k fold and length-N DFT (sm_100a).
 //
 // jht (healpix.py:280-355) groups rings by length and emits one FFT per distinct
-// length, with scatter-adds for the m -> k fold.  Here one CTA owns one ring:
+// length, with scatter-adds for the m -> k fold.  Here a CTA owns a ring (or a piece of one):
 //   synthesis  D[k] = sum_{m = k mod N} Fp_m e^{i m phi0} + sum_{m>=1, -m = k mod N} conj(Fm_m e^{i m phi0})
 //              out[j] = sum_k D[k] e^{+2 pi i jk/N}      (real part: spin 0; Q + iU: spin 2)
 //   adjoint    W[k] = sum_j v[j] e^{-2 pi i jk/N};  V[m] = W[m mod N] e^{-i m phi0}
 //              (spin 2 also Vm[m] = conj(W[-m mod N]) e^{-i m phi0})
 // The fold is a gather (each k collects its own m's), never a scatter.  Power-of-two
 // rings use an in-place Stockham FFT in shared memory (radix-16 passes held in
-// registers, natural order in and out, a padded layout against bank conflicts), in
-// Q = N / 4096 pieces by output residue when N > 4096 (the 4 nside belt rings at
-// nside >= 2048), so a CTA needs 70 KB of shared memory and two fit on an SM; every
-// other length uses
-// Bluestein's chirp-z with an exact (n^2 mod 2N) chirp argument (_azimuth.py:150-191)
-// at a power-of-two length P >= 2N-1, split into Q = P/4096 shared-memory pieces when
-// P > 4096 (decimation in frequency on the input, twiddled recombination on the output).
+// registers, natural order in and out, a padded layout against bank conflicts; 70 KB of
+// shared memory per CTA, two CTAs per SM); every other length uses Bluestein's chirp-z
+// with an exact (n^2 mod 2N) chirp argument (_azimuth.py:150-191) at a power-of-two length
+// P >= 2N-1.  Rings whose transform exceeds 4096 points run as independent pieces, one CTA
+// per output residue class (decimation in frequency on the input, no data exchange): the
+// power-of-two belt rings in N / 4096 pieces and the long polar-cap rings (N = 4 qn) as four
+// chirp-z pieces of length qn; only chirp-z lengths above 16384 (cap rings at nside > 2048)
+// are split inside one CTA through the ring's scratch rows.
 #include <cuda_runtime.h>
 
 #include "jhtb_internal.cuh"
