@@ -262,10 +262,12 @@ int jhtb_plan_inject_fault(jhtb_plan *plan, int kind);
  * elements) and writes out[o * out_dist_outer + t * out_dist_inner + k * out_stride] =
  * scale * w_k * sum_i x[i] e^{sign 2 pi i i k / n}, with w_k = e^{sign 2 pi i (t k mod
  * twiddle_n) / twiddle_n} when twiddle_n > 0 (the four-step twiddle), else 1.  sign = -1
- * (forward) or +1.  In place (out == in) only with the same input and output layout. */
+ * (forward) or +1.  roots: device table of e^{-2 pi i k / n} for k < n (complex128), or NULL
+ * to compute each butterfly's root.  In place (out == in) only with the same input and
+ * output layout. */
 int jhtb_fft_c2c(const void *in, void *out, int n, int64_t howmany, int64_t inner, int64_t in_stride,
                  int64_t in_dist_outer, int64_t in_dist_inner, int64_t out_stride, int64_t out_dist_outer,
-                 int64_t out_dist_inner, int sign, double scale, int64_t twiddle_n, void *stream);
+                 int64_t out_dist_inner, int sign, double scale, int64_t twiddle_n, const void *roots, void *stream);
 
 /* Bounds-check record of a debug library (no counterpart in jht; the replacement for a
  * memory checker on machines where none can run).  A library built with `make debug`

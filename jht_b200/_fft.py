@@ -8,6 +8,9 @@ shared memory up to SM_MAX points and composed from two batched calls (four-step
 
 from __future__ import annotations
 
+from functools import lru_cache
+
+import numpy as np
 import torch
 
 from . import _lib
@@ -39,10 +42,22 @@ def _split(n: int) -> tuple[int, int]:
     return best
 
 
+@lru_cache(maxsize=None)
+def _roots(n: int, device: int) -> torch.Tensor:
+    """e^{-2 pi i k / n}, k < n, on the device (cos and sin of an exactly reduced angle)."""
+    k = np.arange(n)
+    r = np.minimum(k, n - k)  # the angle's magnitude folded to [0, pi]
+    ang = 2.0 * np.pi * r / n
+    z = np.cos(ang) - 1j * np.where(k <= n // 2, 1.0, -1.0) * np.sin(ang)
+    return torch.as_tensor(z, dtype=torch.complex128, device=torch.device("cuda", device))
+
+
 def _call(x, out, n, howmany, inner, in_stride, in_do, in_di, out_stride, out_do, out_di, sign, scale, tw):
     lib = _lib.load_library()
+    roots = _roots(n, x.device.index)
     _lib.check(lib.jhtb_fft_c2c(x.data_ptr(), out.data_ptr(), n, howmany, inner, in_stride, in_do, in_di, out_stride,
-                                out_do, out_di, sign, float(scale), tw, _lib.stream_ptr()), "jhtb_fft_c2c")
+                                out_do, out_di, sign, float(scale), tw, roots.data_ptr(), _lib.stream_ptr()),
+               "jhtb_fft_c2c")
 
 
 def fft(x: torch.Tensor, dim: int, sign: int, scale: float = 1.0) -> torch.Tensor:

@@ -126,7 +126,7 @@ def load_library(path: str | os.PathLike | None = None):
             "jhtb_debug_bounds": (i32, [ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i64),
                                         ctypes.POINTER(i64)]),
             "jhtb_fft_c2c": (i32, [vp, vp, i32, i64, i64, i64, i64, i64, i64, i64, i64, i32, ctypes.c_double, i64,
-                                   vp]),
+                                   vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)

@@ -8,7 +8,8 @@
 // butterfly writes back where it read, so a thread holds one butterfly at a time), and is
 // written back in natural order, optionally scaled and multiplied by a four-step twiddle.  Lengths up to kFftSmMax run in
 // one CTA; the host composes longer ones from two batched calls (four-step).  Every
-// butterfly's twiddle is one sincospi of an exactly reduced rational argument.
+// butterfly's root comes from the caller's table of the n-th roots of unity (or, without a
+// table, from one sincospi of an exactly reduced rational argument).
 //
 // Batch index b = outer * inner_count + t: the transform reads in[o * in_dist_outer +
 // t * in_dist_inner + i * in_stride] for i < n and writes out[...] likewise with the out
@@ -36,6 +37,7 @@ struct FftArgs {
     int sign;
     double scale;
     long long tw_n;  // 0: none; else output k of inner index t times e^{sign 2 pi i (t k mod tw_n) / tw_n}
+    const double2 *roots;  // e^{-2 pi i k / n} for k < n, or null (each butterfly's root by sincospi)
 };
 
 __device__ __forceinline__ double2 f_cmul(double2 a, double2 b) {
@@ -103,11 +105,12 @@ __device__ __forceinline__ void small_dft<5>(double2 (&v)[5], double sgn) {
 // One in-place decimation-in-time stage of radix R over n points that hold sub-transforms
 // of length m (natural order within each): butterfly (g, j), g a multiple of L = m R and
 // j < m, combines the R elements g + j + q m (q < R) after twiddling element q by
-// w^q, w = e^{sgn 2 pi i j / L} (one sincospi per butterfly, its powers by multiplication),
+// w^q, w = e^{sgn 2 pi i j / L} (one table entry per butterfly, its powers by multiplication),
 // and stores them back in place, so a thread holds only R values at a time.
 template <int R>
-__device__ __forceinline__ void dit_stage(double2 *buf, int n, int m, double sgn) {
+__device__ __forceinline__ void dit_stage(double2 *buf, int n, int m, double sgn, const double2 *__restrict__ roots) {
     const int L = m * R, nb = n / R;
+    const int rstep = n / L;  // e^{-2 pi i j / L} = roots[j n / L]
     for (int bi = threadIdx.x; bi < nb; bi += kFftSmThreads) {
         const int gq = bi / m, j = bi - gq * m;
         const int base = gq * L + j;
@@ -115,7 +118,13 @@ __device__ __forceinline__ void dit_stage(double2 *buf, int n, int m, double sgn
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = buf[base + q * m];
         if (m > 1) {
-            const double2 w = f_root(j, L, sgn);
+            double2 w;
+            if (roots) {
+                w = __ldg(&roots[j * rstep]);
+                w.y *= -sgn;  // the table holds e^{-2 pi i k / n}
+            } else {
+                w = f_root(j, L, sgn);
+            }
             double2 wq = w;
 #pragma unroll
             for (int q = 1; q < R; ++q) {
@@ -153,10 +162,10 @@ __global__ void __launch_bounds__(kFftSmThreads, 1) fft_smooth_kernel(FftArgs a)
             fbuf[digit_reversed(i, n, a.c4, a.c2, a.c3, a.c5)] = src[(long long)i * a.in_stride];
         __syncthreads();
         int m = 1;
-        for (int p = 0; p < a.c4; ++p, m *= 4) dit_stage<4>(fbuf, n, m, sgn);
-        for (int p = 0; p < a.c2; ++p, m *= 2) dit_stage<2>(fbuf, n, m, sgn);
-        for (int p = 0; p < a.c3; ++p, m *= 3) dit_stage<3>(fbuf, n, m, sgn);
-        for (int p = 0; p < a.c5; ++p, m *= 5) dit_stage<5>(fbuf, n, m, sgn);
+        for (int p = 0; p < a.c4; ++p, m *= 4) dit_stage<4>(fbuf, n, m, sgn, a.roots);
+        for (int p = 0; p < a.c2; ++p, m *= 2) dit_stage<2>(fbuf, n, m, sgn, a.roots);
+        for (int p = 0; p < a.c3; ++p, m *= 3) dit_stage<3>(fbuf, n, m, sgn, a.roots);
+        for (int p = 0; p < a.c5; ++p, m *= 5) dit_stage<5>(fbuf, n, m, sgn, a.roots);
         double2 *dst = a.out + o * a.out_dist_outer + t * a.out_dist_inner;
         for (int k = threadIdx.x; k < n; k += kFftSmThreads) {
             double2 v = fbuf[k];
@@ -176,7 +185,8 @@ using namespace jhtb;
 
 extern "C" int jhtb_fft_c2c(const void *in, void *out, int n, int64_t howmany, int64_t inner, int64_t in_stride,
                             int64_t in_dist_outer, int64_t in_dist_inner, int64_t out_stride, int64_t out_dist_outer,
-                            int64_t out_dist_inner, int sign, double scale, int64_t twiddle_n, void *stream) {
+                            int64_t out_dist_inner, int sign, double scale, int64_t twiddle_n, const void *roots,
+                            void *stream) {
     if (!in || !out) return fail(JHTB_ERR_INVALID, "jhtb_fft_c2c: NULL argument");
     if (n < 1 || n > kFftSmMax)
         return fail(JHTB_ERR_INVALID, "jhtb_fft_c2c: n must be in [1, " + std::to_string(kFftSmMax) + "], got " +
@@ -207,6 +217,7 @@ extern "C" int jhtb_fft_c2c(const void *in, void *out, int n, int64_t howmany, i
     a.sign = sign;
     a.scale = scale;
     a.tw_n = twiddle_n;
+    a.roots = (const double2 *)roots;
     if (howmany == 0) return JHTB_OK;
     const int smem = n * (int)sizeof(double2);
     JHTB_CUDA_TRY(cudaFuncSetAttribute(fft_smooth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

@@ -57,6 +57,22 @@ def test_four_step_matches_numpy(n, dim):
         assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= TOL, (n, dim, sign)
 
 
+@pytest.mark.parametrize("n", [60, 8640, 17280])
+def test_fft_without_a_roots_table(n, monkeypatch):
+    """A NULL roots table: each butterfly computes its root (one sincospi)."""
+
+    class _Null:
+        def data_ptr(self):
+            return 0
+
+    monkeypatch.setattr(_fft, "_roots", lambda n, device: _Null())
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((3, n)) + 1j * rng.standard_normal((3, n))
+    got = _fft.fft(torch.as_tensor(x, device="cuda"), 1, -1).cpu().numpy()
+    ref = _ref(x, 1, -1, 1.0)
+    assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) <= TOL
+
+
 def test_fft_rejects_unsupported_lengths():
     x = torch.zeros((7, 3), dtype=torch.complex128, device="cuda")
     with pytest.raises(ValueError, match="smooth"):

@@ -303,11 +303,11 @@ def test_fft_split_and_argument_checks(lib):
         assert n1 * n2 == n and n1 <= _fft.SM_MAX and n2 <= _fft.SM_MAX
         assert _fft._smooth(n1) and _fft._smooth(n2)
     buf = ctypes.c_void_p(16)
-    args = (1, 1, 1, 1, 0, 1, 1, 0, -1, 1.0, 0, None)
+    args = (1, 1, 1, 1, 0, 1, 1, 0, -1, 1.0, 0, None, None)
     assert lib.jhtb_fft_c2c(buf, buf, 7, *args) == _lib.JHTB_ERR_INVALID      # not 2,3,5-smooth
     assert "smooth" in _lib.last_error()
     assert lib.jhtb_fft_c2c(buf, buf, 20480, *args) == _lib.JHTB_ERR_INVALID  # above the shared-memory limit
-    assert lib.jhtb_fft_c2c(buf, buf, 8, 1, 1, 1, 1, 0, 1, 1, 0, 2, 1.0, 0, None) == _lib.JHTB_ERR_INVALID  # sign
+    assert lib.jhtb_fft_c2c(buf, buf, 8, 1, 1, 1, 1, 0, 1, 1, 0, 2, 1.0, 0, None, None) == _lib.JHTB_ERR_INVALID  # sign
     assert lib.jhtb_fft_c2c(None, buf, 8, *args) == _lib.JHTB_ERR_INVALID
 
 
