@@ -42,14 +42,34 @@ def _split(n: int) -> tuple[int, int]:
     return best
 
 
+_PI_LD = np.longdouble("3.14159265358979323846264338327950288")
+
+
+def _roots_host(n: int) -> np.ndarray:
+    """e^{-2 pi i k / n} for k < n as complex128.  The angle is folded to the first octant in
+    integers: with r = min(k, n - k) it is pi b / (2 n), b = 4 r in [0, 2 n]; b > n reflects
+    about pi / 2 (the cosine changes sign), then 2 b > n about pi / 4 (cosine and sine swap).
+    The octant's cosine and sine are taken in the host's extended precision (x86: 64-bit
+    mantissa) before rounding to FP64, so each entry is within about half an FP64 ulp, and
+    the multiples of pi / 2 come out exactly."""
+    k = np.arange(n, dtype=np.int64)
+    b = 4 * np.minimum(k, n - k)
+    flip = b > n
+    b = np.where(flip, 2 * n - b, b)
+    swap = 2 * b > n
+    b = np.where(swap, n - b, b)
+    ang = _PI_LD * b.astype(np.longdouble) / (2 * n)
+    c, s = np.cos(ang).astype(np.float64), np.sin(ang).astype(np.float64)
+    c, s = np.where(swap, s, c), np.where(swap, c, s)
+    c = np.where(flip, -c, c)
+    s = np.where(k <= n // 2, s, -s)
+    return c - 1j * s
+
+
 @lru_cache(maxsize=None)
 def _roots(n: int, device: int) -> torch.Tensor:
-    """e^{-2 pi i k / n}, k < n, on the device (cos and sin of an exactly reduced angle)."""
-    k = np.arange(n)
-    r = np.minimum(k, n - k)  # the angle's magnitude folded to [0, pi]
-    ang = 2.0 * np.pi * r / n
-    z = np.cos(ang) - 1j * np.where(k <= n // 2, 1.0, -1.0) * np.sin(ang)
-    return torch.as_tensor(z, dtype=torch.complex128, device=torch.device("cuda", device))
+    """The table of _roots_host(n) on the device (built once per length and device)."""
+    return torch.as_tensor(_roots_host(n), dtype=torch.complex128, device=torch.device("cuda", device))
 
 
 def _call(x, out, n, howmany, inner, in_stride, in_do, in_di, out_stride, out_do, out_di, sign, scale, tw):

@@ -366,3 +366,25 @@ def test_fft_four_step_composition_on_a_model_of_the_kernel(monkeypatch):
             got = _fft.fft(T(x), dim, sign, 0.5).a
             ref = (np.fft.fft(x, axis=dim) if sign < 0 else np.fft.ifft(x, axis=dim) * n) * 0.5
             assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-12, (n, dim, sign)
+
+
+def test_fft_roots_table_against_a_40_digit_reference():
+    """The FFT kernel's table of roots of unity: exact symmetries, and each sampled entry
+    within one FP64 ulp of e^{-2 pi i k / n} taken at 40 digits."""
+    mpmath = pytest.importorskip("mpmath")
+    from jht_b200 import _fft
+
+    mpmath.mp.dps = 40
+    for n in (1, 2, 3, 243, 625, 8640, 10240):
+        z = _fft._roots_host(n)
+        assert z.shape == (n,) and z.dtype == np.complex128 and z[0] == 1.0
+        k = np.arange(1, n)
+        assert np.array_equal(z[n - k], np.conj(z[k]))
+        if n % 2 == 0:
+            assert z[n // 2] == -1.0
+        if n % 4 == 0:
+            assert z[n // 4] == -1j and z[3 * n // 4] == 1j
+        ks = np.unique(np.r_[np.arange(0, n, max(1, n // 499)), n - 1])
+        ref = np.array([complex(mpmath.cos(2 * mpmath.pi * int(j) / n), -mpmath.sin(2 * mpmath.pi * int(j) / n))
+                        for j in ks])
+        assert np.max(np.abs(z[ks] - ref)) <= 1.2e-16, n
