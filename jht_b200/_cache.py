@@ -12,6 +12,6 @@ __all__ = ["enable_compilation_cache"]
 _settings: dict[str, object] = {}
 
 
-def enable_compilation_cache(cache_dir: str | None = None, min_compile_time_secs: float = 1.0) -> None:
-    _settings["cache_dir"] = cache_dir
+def enable_compilation_cache(directory: str, *, min_compile_time_secs: float = 1.0) -> None:
+    _settings["directory"] = directory
     _settings["min_compile_time_secs"] = float(min_compile_time_secs)

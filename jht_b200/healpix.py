@@ -254,13 +254,13 @@ def synthesis(alm, nside: int, lmax: int, spin: int = 0, *, precision: str = "fp
     return out.reshape((12 * nside * nside,) if spin == 0 else (2, 12 * nside * nside))
 
 
-def adjoint_synthesis(maps, nside: int, lmax: int, spin: int = 0, *, precision: str = "fp64") -> torch.Tensor:
+def adjoint_synthesis(m, nside: int, lmax: int, spin: int = 0, *, precision: str = "fp64") -> torch.Tensor:
     """``S^T``: the exact transpose of :func:`synthesis` (healpix.py:390-412).
 
     ``<S a, v>_map == sum (2 - delta_m0) Re(conj(a) S^T v)``; equals
     ``(Npix / 4 pi) healpy.map2alm(v, iter=0)``.  Input ``(Npix,)`` or ``(2, Npix)``.
     """
-    m = _as_map(maps)
+    m = _as_map(m)
     npix = 12 * nside * nside
     expect = (npix,) if spin == 0 else (2, npix)
     if tuple(m.shape) != expect:

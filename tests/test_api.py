@@ -41,3 +41,73 @@ def test_reexports_are_the_implementations():
     assert jhtb.synthesis_real is diff.synthesis_real
     assert jhtb.synthesis_general_real is diff.synthesis_general_real
     assert jhtb.alm_to_real is masked.alm_to_real
+
+
+_REQ = object()  # no default
+
+# jht v0.2.0's signatures: name -> (positional parameters with defaults, keyword-only parameters
+# with defaults); the source line of each def is given beside it.
+JHT_SIGNATURES = {
+    "synthesis": ({"alm": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0}, {}),  # healpix.py:363
+    "adjoint_synthesis": ({"m": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0}, {}),  # healpix.py:390
+    "synthesis_general": ({"alm": _REQ, "loc": _REQ}, {"spin": 0, "lmax": _REQ, "epsilon": 1e-10}),  # offgrid.py:172
+    "adjoint_synthesis_general": ({"field": _REQ, "loc": _REQ},
+                                  {"spin": 0, "lmax": _REQ, "epsilon": 1e-10}),  # offgrid.py:215
+    "analysis": ({"maps": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0, "niter": 3, "use_weights": True},
+                 {}),  # _analysis.py:55
+    "bare_analysis": ({"maps": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0, "use_weights": True},
+                      {}),  # _analysis.py:49
+    "ring_weights": ({"nside": _REQ}, {}),  # weights.py:61
+    "pixel_weights": ({"nside": _REQ, "use_weights": True}, {}),  # weights.py:87
+    "pseudo_alm": ({"maps": _REQ, "mask": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0, "niter": 3,
+                    "use_weights": True}, {}),  # masked.py:99
+    "deconvolve": ({"maps": _REQ, "mask": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0},
+                   {"max_iter": 200, "tol": 1e-8, "reg": 0.0, "use_weights": True, "x0": None}),  # masked.py:278
+    "wiener": ({"maps": _REQ, "signal_cl": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0},
+               {"inv_noise": None, "mask": None, "max_iter": 200, "tol": 1e-8, "use_weights": True,
+                "x0": None}),  # masked.py:320
+    "constrained_realization": ({"maps": _REQ, "signal_cl": _REQ, "nside": _REQ, "lmax": _REQ, "key": _REQ,
+                                 "spin": 0},
+                                {"inv_noise": None, "mask": None, "max_iter": 200, "tol": 1e-8,
+                                 "use_weights": True, "x0": None}),  # masked.py:374
+    "synthesis_real": ({"x": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0}, {}),  # diff.py:55
+    "analysis_real": ({"maps": _REQ, "nside": _REQ, "lmax": _REQ, "spin": 0, "niter": 3, "use_weights": True},
+                      {}),  # diff.py:64
+    "synthesis_general_real": ({"x": _REQ, "loc": _REQ}, {"spin": 0, "lmax": _REQ, "epsilon": 1e-10}),  # diff.py:79
+    "adjoint_synthesis_general_real": ({"field": _REQ, "loc": _REQ},
+                                       {"spin": 0, "lmax": _REQ, "epsilon": 1e-10}),  # diff.py:95
+    "bandpower": ({"alm": _REQ, "lmax": _REQ, "spin": 0}, {}),  # diff.py:119
+    "alm_to_real": ({"alm": _REQ, "lmax": _REQ, "spin": 0}, {}),  # masked.py:160
+    "real_to_alm": ({"x": _REQ, "lmax": _REQ, "spin": 0}, {}),  # masked.py:169
+    "n_dof": ({"lmax": _REQ, "spin": 0}, {}),  # masked.py:140
+    "alm_size": ({"lmax": _REQ}, {}),  # healpix.py:49
+    "alm_metric_weight": ({"lmax": _REQ}, {}),  # healpix.py:59
+    "enable_compilation_cache": ({"directory": _REQ}, {"min_compile_time_secs": 1.0}),  # _cache.py:25
+    "set_azimuth_fft_mode": ({"mode": _REQ}, {}),  # _azimuth.py:60
+    "get_azimuth_fft_mode": ({}, {}),  # _azimuth.py:82
+    "enable_looped_fft": ({}, {}),  # _azimuth.py:87
+}
+
+
+def test_signatures_match_jht():
+    """Every jht call still binds: the same positional parameters in the same order with the
+    same defaults, the same keyword-only parameters with the same defaults.  Additions are
+    allowed only as keyword-only parameters with a default (``precision``)."""
+    import inspect
+
+    sigs = dict(JHT_SIGNATURES, map2alm=JHT_SIGNATURES["analysis"])  # an alias of analysis in jht (_analysis.py:67)
+    assert set(sigs) == JHT_SURFACE
+    for name, (pos, kw) in sigs.items():
+        params = inspect.signature(getattr(jhtb, name)).parameters.values()
+        got_pos = {p.name: (_REQ if p.default is p.empty else p.default) for p in params
+                   if p.kind in (p.POSITIONAL_ONLY, p.POSITIONAL_OR_KEYWORD)}
+        got_kw = {p.name: (_REQ if p.default is p.empty else p.default) for p in params
+                  if p.kind == p.KEYWORD_ONLY}
+        assert list(got_pos) == list(pos), name
+        for k, d in pos.items():
+            assert got_pos[k] is d if d is _REQ else got_pos[k] == d, (name, k)
+        for k, d in kw.items():
+            assert k in got_kw, (name, k)
+            assert got_kw[k] is d if d is _REQ else got_kw[k] == d, (name, k)
+        for k in set(got_kw) - set(kw):
+            assert got_kw[k] is not _REQ, (name, k)
