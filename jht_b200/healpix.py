@@ -118,18 +118,21 @@ def _device() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
+def _host_tensor(x) -> torch.Tensor:
+    """``x`` as a tensor where it lies (array-likes wrap host memory without a copy), so
+    shapes are checked before any device transfer."""
+    return x if isinstance(x, torch.Tensor) else torch.as_tensor(np.asarray(x))
+
+
 def _as_alm(alm) -> torch.Tensor:
-    if isinstance(alm, torch.Tensor):
-        t = alm
-    else:
-        t = torch.as_tensor(np.asarray(alm))
+    t = _host_tensor(alm)
     if not t.is_complex():
         t = t.to(torch.float64)
     return t.to(device=_device(), dtype=torch.complex128)
 
 
 def _as_map(m) -> torch.Tensor:
-    t = m if isinstance(m, torch.Tensor) else torch.as_tensor(np.asarray(m))
+    t = _host_tensor(m)
     if t.is_complex():
         raise TypeError("maps must be real")
     return t.to(device=_device(), dtype=torch.float64)
@@ -241,7 +244,7 @@ def synthesis(alm, nside: int, lmax: int, spin: int = 0, *, precision: str = "fp
     (E, B) for spin 2.  Returns ``(12 nside^2,)`` or ``(2, 12 nside^2)`` (Q, U).
     ``precision`` selects the contraction arithmetic ("fp64" plain or "fp32").
     """
-    a = _as_alm(alm)
+    a = _host_tensor(alm)
     expect = (alm_size(lmax),) if spin == 0 else (2, alm_size(lmax))
     if tuple(a.shape) != expect:
         raise ValueError(
@@ -250,6 +253,7 @@ def synthesis(alm, nside: int, lmax: int, spin: int = 0, *, precision: str = "fp
         )
     _check_spin(spin)
     _ceiling_warning(nside, lmax, spin)
+    a = _as_alm(a)
     out = _Synthesis.apply(a.reshape(1, -1, alm_size(lmax)), nside, lmax, spin, precision)
     return out.reshape((12 * nside * nside,) if spin == 0 else (2, 12 * nside * nside))
 
@@ -260,7 +264,7 @@ def adjoint_synthesis(m, nside: int, lmax: int, spin: int = 0, *, precision: str
     ``<S a, v>_map == sum (2 - delta_m0) Re(conj(a) S^T v)``; equals
     ``(Npix / 4 pi) healpy.map2alm(v, iter=0)``.  Input ``(Npix,)`` or ``(2, Npix)``.
     """
-    m = _as_map(m)
+    m = _host_tensor(m)
     npix = 12 * nside * nside
     expect = (npix,) if spin == 0 else (2, npix)
     if tuple(m.shape) != expect:
@@ -270,6 +274,7 @@ def adjoint_synthesis(m, nside: int, lmax: int, spin: int = 0, *, precision: str
         )
     _check_spin(spin)
     _ceiling_warning(nside, lmax, spin)
+    m = _as_map(m)
     out = _Adjoint.apply(m.reshape(1, -1, npix), nside, lmax, spin, precision)
     return out.reshape((alm_size(lmax),) if spin == 0 else (2, alm_size(lmax)))
 

@@ -36,7 +36,15 @@ import torch
 
 from . import _lib
 from . import _fft
-from .healpix import _adjoint_cotangent_input, _as_alm, _device, _synthesis_cotangent, alm_metric_weight, alm_size
+from .healpix import (
+    _adjoint_cotangent_input,
+    _as_alm,
+    _device,
+    _host_tensor,
+    _synthesis_cotangent,
+    alm_metric_weight,
+    alm_size,
+)
 
 __all__ = ["synthesis_general", "adjoint_synthesis_general"]
 
@@ -322,10 +330,11 @@ class _AdjointGeneral(torch.autograd.Function):
 # public API
 # ---------------------------------------------------------------------------------------
 def _check_loc(loc) -> torch.Tensor:
-    t = loc if isinstance(loc, torch.Tensor) else torch.as_tensor(np.asarray(loc))
+    """``loc`` as a tensor where it lies, its shape checked (moved to the device later)."""
+    t = _host_tensor(loc)
     if t.dim() != 2 or t.shape[-1] != 2:
         raise ValueError(f"loc must have shape (npts, 2) [theta, phi]; got {tuple(t.shape)}")
-    return t.to(device=_device(), dtype=torch.float64)
+    return t
 
 
 def _check_spin(spin: int) -> None:
@@ -345,13 +354,15 @@ def synthesis_general(alm, loc, *, spin: int = 0, lmax: int, epsilon: float = 1e
     """
     _check_spin(spin)
     t = _check_loc(loc)
-    a = _as_alm(alm)
+    a = _host_tensor(alm)
     expect = (alm_size(lmax),) if spin == 0 else (2, alm_size(lmax))
     if tuple(a.shape) != expect:
         raise ValueError(
             f"alm shape {tuple(a.shape)} != expected {expect} for lmax={lmax}, spin={spin} "
             "(a wrong-size alm would otherwise be silently clamped by the gather)"
         )
+    a = _as_alm(a)
+    t = t.to(device=a.device, dtype=torch.float64)
     g = _geometry(int(lmax), int(spin), float(epsilon), a.device.index)
     theta, phi = t[:, 0].contiguous(), t[:, 1].contiguous()
     return _SynthesisGeneral.apply(a.reshape(g.ncomp, -1), theta, phi, g)
@@ -362,7 +373,7 @@ def adjoint_synthesis_general(field, loc, *, spin: int = 0, lmax: int, epsilon: 
     (offgrid.py:223-243).  ``field``: real ``(npts,)`` (spin 0) or ``(2, npts)`` (Q, U)."""
     _check_spin(spin)
     t = _check_loc(loc)
-    f = field if isinstance(field, torch.Tensor) else torch.as_tensor(np.asarray(field))
+    f = _host_tensor(field)
     if f.is_complex():
         raise TypeError(
             "field must be real ((npts,) for spin=0; (2, npts) real Q/U planes for spin>0); "
@@ -372,6 +383,7 @@ def adjoint_synthesis_general(field, loc, *, spin: int = 0, lmax: int, epsilon: 
     expect = (npts,) if spin == 0 else (2, npts)
     if tuple(f.shape) != expect:
         raise ValueError(f"field shape {tuple(f.shape)} != expected {expect} for {npts} points")
+    t = t.to(device=_device(), dtype=torch.float64)
     f = f.to(device=t.device, dtype=torch.float64).contiguous()
     g = _geometry(int(lmax), int(spin), float(epsilon), t.device.index)
     theta, phi = t[:, 0].contiguous(), t[:, 1].contiguous()

@@ -111,3 +111,53 @@ def test_signatures_match_jht():
             assert got_kw[k] is d if d is _REQ else got_kw[k] == d, (name, k)
         for k in set(got_kw) - set(kw):
             assert got_kw[k] is not _REQ, (name, k)
+
+
+def test_input_validation_before_device_work():
+    """Wrong-size inputs raise jht's errors (tests/test_healpix.py:138-149 and
+    tests/test_diff_offgrid.py:138-151 of jht) before any device work, so they read the
+    same on a host without a GPU."""
+    import numpy as np
+    import pytest
+
+    nside, lmax = 16, 24
+    K = jhtb.alm_size(lmax)
+    with pytest.raises(ValueError, match="alm shape"):
+        jhtb.synthesis(np.zeros(K - 1, dtype=np.complex128), nside, lmax, spin=0)
+    with pytest.raises(ValueError, match="alm shape"):
+        jhtb.synthesis(np.zeros(K, dtype=np.complex128), nside, lmax, spin=2)  # missing (2, K)
+    with pytest.raises(ValueError, match="map shape"):
+        jhtb.adjoint_synthesis(np.zeros(12 * nside**2 - 1), nside, lmax, spin=0)
+    with pytest.raises(ValueError, match="map shape"):
+        jhtb.adjoint_synthesis(np.zeros(12 * nside**2), nside, lmax, spin=2)  # missing (2, npix)
+
+    L = 8
+    rng = np.random.default_rng(700)
+    loc = np.stack([rng.uniform(0, np.pi, 10), rng.uniform(0, 2 * np.pi, 10)], axis=1)
+    alm = np.zeros(jhtb.alm_size(L), dtype=np.complex128)
+    with pytest.raises(ValueError, match="alm shape"):
+        jhtb.synthesis_general(np.zeros(3, dtype=complex), loc, spin=0, lmax=L)
+    with pytest.raises(ValueError, match="loc must"):
+        jhtb.synthesis_general(alm, loc[:, :1], spin=0, lmax=L)
+    with pytest.raises(ValueError, match="field shape"):
+        jhtb.adjoint_synthesis_general(np.zeros(9), loc, spin=0, lmax=L)
+    with pytest.raises(ValueError, match="field shape"):
+        jhtb.adjoint_synthesis_general(np.zeros(10), loc, spin=2, lmax=L)  # missing (2, npts)
+    with pytest.raises(TypeError, match="real"):
+        jhtb.adjoint_synthesis_general(np.zeros(10, dtype=complex), loc, spin=0, lmax=L)
+
+
+def test_band_ceiling_warning_before_device_work():
+    """lmax > 1.5 nside warns once per geometry (jht tests/test_healpix.py:152-160); on a host
+    without a GPU the call then fails loudly instead of falling back to the CPU."""
+    import contextlib
+
+    import numpy as np
+    import pytest
+    import torch
+
+    a = np.zeros(jhtb.alm_size(8), dtype=np.complex128)  # 8 > 1.5 * 5; a geometry no other test uses
+    no_gpu = not torch.cuda.is_available()
+    with pytest.warns(UserWarning, match="ceiling"):
+        with pytest.raises(RuntimeError, match="CUDA") if no_gpu else contextlib.nullcontext():
+            jhtb.synthesis(a, 5, 8, spin=0)
