@@ -161,3 +161,19 @@ def test_band_ceiling_warning_before_device_work():
     with pytest.warns(UserWarning, match="ceiling"):
         with pytest.raises(RuntimeError, match="CUDA") if no_gpu else contextlib.nullcontext():
             jhtb.synthesis(a, 5, 8, spin=0)
+
+
+def test_azimuth_mode_toggle_validation():
+    """jht tests/test_azimuth_fft.py:224-228: a bad mode raises and leaves the mode unchanged;
+    the shortcut selects "looped".  (Both modes run the same ring kernels here.)"""
+    import pytest
+
+    assert jhtb.get_azimuth_fft_mode() == "unrolled"
+    with pytest.raises(ValueError, match="unknown azimuth FFT mode"):
+        jhtb.set_azimuth_fft_mode("bogus")
+    assert jhtb.get_azimuth_fft_mode() == "unrolled"
+    try:
+        jhtb.enable_looped_fft()
+        assert jhtb.get_azimuth_fft_mode() == "looped"
+    finally:
+        jhtb.set_azimuth_fft_mode("unrolled")

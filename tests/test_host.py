@@ -388,3 +388,42 @@ def test_fft_roots_table_against_a_40_digit_reference():
         ref = np.array([complex(mpmath.cos(2 * mpmath.pi * int(j) / n), -mpmath.sin(2 * mpmath.pi * int(j) / n))
                         for j in ks])
         assert np.max(np.abs(z[ks] - ref)) <= 1.2e-16, n
+
+
+def _quadrature_moments(nside):
+    """Q_l = sum over pixels of W_pix P_l(z_pix), l <= 2 nside, summed ring by ring (every
+    pixel of a ring has the same z)."""
+    from numpy.polynomial.legendre import legvander
+
+    from jht_b200.healpix import RingInfo
+
+    geo = RingInfo(nside)
+    ring_w = np.add.reduceat(weights.pixel_weights(nside), geo.startpix)
+    return ring_w @ legvander(geo.z, 2 * nside)
+
+
+@pytest.mark.parametrize("nside", [2, 4, 8, 16, 32, 64, 128, 256, 512, 2048])
+def test_ring_weight_properties(nside):
+    """jht tests/test_weights.py:40-68: the ring weights are small corrections to 1, and with
+    them the m = 0 quadrature integrates P_l exactly for even l <= 2 nside (Q_0 = 4 pi, the
+    higher even moments vanish); up to the benchmark's nside 2048."""
+    w = weights.ring_weights(nside)
+    assert w.shape == (2 * nside,) and np.all(np.isfinite(w)) and np.max(np.abs(w)) < 0.5
+    q = _quadrature_moments(nside)
+    assert abs(q[0] - 4 * np.pi) < 1e-12 * 4 * np.pi
+    assert np.max(np.abs(q[2::2])) < 1e-12 * 4 * np.pi
+
+
+def test_pixel_weight_properties():
+    """jht tests/test_weights.py:70-89: the pixel weights sum to 4 pi (with and without the
+    ring weights), and a southern ring's pixels carry its northern partner's weight."""
+    from jht_b200.healpix import RingInfo
+
+    for nside in (4, 16, 64, 256):
+        assert abs(weights.pixel_weights(nside).sum() - 4 * np.pi) < 1e-11
+        w0 = weights.pixel_weights(nside, use_weights=False)
+        assert np.allclose(w0, 4 * np.pi / (12 * nside**2)) and abs(w0.sum() - 4 * np.pi) < 1e-12
+    nside = 32
+    geo, wv = RingInfo(nside), weights.pixel_weights(nside)
+    for r in (0, 5, 2 * nside - 2):
+        assert abs(wv[geo.startpix[r]] - wv[geo.startpix[4 * nside - 2 - r]]) < 1e-15
