@@ -427,3 +427,40 @@ def test_pixel_weight_properties():
     geo, wv = RingInfo(nside), weights.pixel_weights(nside)
     for r in (0, 5, 2 * nside - 2):
         assert abs(wv[geo.startpix[r]] - wv[geo.startpix[4 * nside - 2 - r]]) < 1e-15
+
+
+def _rand_alm_host(lmax, spin, seed):
+    rng = np.random.default_rng(seed)
+    ell, _ = O.lm_of_index(lmax)
+    out = []
+    for _ in range(2 if spin == 2 else 1):
+        a = rng.standard_normal(ell.size) + 1j * rng.standard_normal(ell.size)
+        a[: lmax + 1] = a[: lmax + 1].real
+        if spin == 2:
+            a[ell < 2] = 0.0
+        out.append(a)
+    return out[0] if spin == 0 else np.stack(out)
+
+
+@pytest.mark.parametrize("spin", [0, 2])
+def test_real_dof_isometry(spin):
+    """jht tests/test_masked.py:125-145: T^-1 T = I on packed a_lm, and ||T a||^2 equals the
+    (2 - delta_m0)-weighted norm of a; n_dof is the length of T a."""
+    lmax = 10
+    a = _rand_alm_host(lmax, spin, 1 + spin)
+    x = masked.alm_to_real(torch.as_tensor(a), lmax, spin)
+    assert x.shape == (jhtb.n_dof(lmax, spin),)
+    back = masked.real_to_alm(x, lmax, spin).numpy()
+    assert np.max(np.abs(back - a)) <= 1e-14
+    w = jhtb.alm_metric_weight(lmax)
+    wnorm2 = float(np.sum(w * np.abs(np.atleast_2d(a)) ** 2))
+    assert abs(float(torch.sum(x * x)) - wnorm2) <= 1e-13 * wnorm2
+
+
+def test_bandpower_on_host_tensors_matches_oracle():
+    """bandpower is plain tensor arithmetic: on host tensors it equals the oracle's C_l."""
+    lmax = 12
+    a = _rand_alm_host(lmax, 0, 9)
+    got = jhtb.bandpower(torch.as_tensor(a), lmax).numpy()
+    ref = O.bandpower(a, lmax)
+    assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
