@@ -33,9 +33,12 @@ GRANULE = 256  # ring ranges are aligned to the tile widths of every kernel
 
 
 def ring_partition(costs, world: int) -> list[tuple[int, int]]:
-    """Split granules 0..len(costs)-1 into `world` contiguous, non-empty-where-possible
-    ranges with near-equal total cost (each boundary at the prefix sum closest to an
-    equal share).  Returns [(g0, g1), ...] in granule units."""
+    """Split granules 0..len(costs)-1 into `world` contiguous ranges with near-equal total
+    cost: boundary r sits at the prefix sum closest to r/world of the total, moved one
+    granule past boundary r-1 if it would not advance (while granules remain).  No range
+    costs more than total/world + the largest granule cost; a range can be empty (an idle
+    rank) when one granule outweighs several shares.  Returns [(g0, g1), ...] in granule
+    units."""
     c = np.asarray(costs, dtype=np.float64)
     n = c.size
     if world < 1:

@@ -35,6 +35,21 @@ def test_partition_is_contiguous_and_balanced():
         assert max(loads) <= costs.sum() / world + costs.max() + 1e-9
 
 
+def test_partition_bound_on_skewed_costs():
+    """The load bound (total/world + the largest granule) also for heavy-tailed and rising
+    costs (the polar-to-equator ring profile), and with one granule outweighing the rest."""
+    rng = np.random.default_rng(1)
+    for it in range(3000):
+        n, world = int(rng.integers(1, 60)), int(rng.integers(1, 12))
+        costs = rng.pareto(1.5, n) + 0.01 if it % 2 else np.linspace(1.0, 3.0, n) ** 2
+        parts = D.ring_partition(costs, world)
+        assert parts[0][0] == 0 and parts[-1][1] == n
+        assert all(a[1] == b[0] and a[0] <= a[1] for a, b in zip(parts, parts[1:]))
+        assert max(costs[g0:g1].sum() for g0, g1 in parts) <= (costs.sum() / world + costs.max()) * (1 + 1e-12)
+    parts = D.ring_partition([1.0, 1.0, 1.0, 100.0], 4)
+    assert max(sum([1.0, 1.0, 1.0, 100.0][g0:g1]) for g0, g1 in parts) == 100.0
+
+
 def test_partition_of_few_granules_leaves_ranks_idle():
     parts = D.ring_partition([1.0, 1.0], 4)
     assert [p for p in parts if p[1] > p[0]] == [(0, 1), (1, 2)]
