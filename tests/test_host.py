@@ -464,3 +464,63 @@ def test_bandpower_on_host_tensors_matches_oracle():
     got = jhtb.bandpower(torch.as_tensor(a), lmax).numpy()
     ref = O.bandpower(a, lmax)
     assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
+
+
+def _fft_kernel_model(x, sign):
+    """The index arithmetic of fft_smooth_kernel (fft.cu) in NumPy: radix counts (4, 2, 3, 5
+    in that order), the mixed-radix digit-reversed load, in-place DIT stages whose butterfly
+    (g, j) twiddles element q by roots[j n / L]^q (sign applied to the table's e^{-2 pi i k/n})
+    before an R-point DFT.  Used to sweep every smooth length; the kernel runs on the GPU."""
+    from jht_b200 import _fft
+
+    n = x.size
+    counts, r = [], n
+    for R in (4, 2, 3, 5):
+        c = 0
+        while r % R == 0:
+            c, r = c + 1, r // R
+        counts.append(c)
+    assert r == 1
+    radices = [R for R, c in zip((4, 2, 3, 5), counts) for _ in range(c)]
+    i = np.arange(n)
+    pos, span, rem = np.zeros(n, dtype=np.int64), n, i.copy()
+    for R in reversed(radices):  # the last stage's radix is the least significant digit
+        span //= R
+        pos += (rem % R) * span
+        rem //= R
+    buf = np.empty(n, dtype=np.complex128)
+    buf[pos] = x
+    roots = _fft._roots_host(n)
+    m = 1
+    for R in radices:
+        L = m * R
+        bi = np.arange(n // R)
+        gq, j = bi // m, bi % m
+        base = gq * L + j
+        v = np.stack([buf[base + q * m] for q in range(R)])
+        w = roots[j * (n // L)]
+        if sign > 0:
+            w = np.conj(w)
+        v = v * w[None, :] ** np.arange(R)[:, None]
+        dft = np.exp(sign * 2j * np.pi * np.outer(np.arange(R), np.arange(R)) / R)
+        v = dft @ v
+        for q in range(R):
+            buf[base + q * m] = v[q]
+        m = L
+    return buf
+
+
+def test_fft_kernel_index_model_for_every_smooth_length():
+    """Every 2,3,5-smooth length up to the shared-memory limit, both signs: the kernel's
+    digit-reversed load and stage indexing compose to the DFT (NumPy's fft)."""
+    from jht_b200 import _fft
+
+    rng = np.random.default_rng(11)
+    lengths = [n for n in range(1, _fft.SM_MAX + 1) if _fft._smooth(n)]
+    assert len(lengths) == 177
+    for n in lengths:
+        x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        for sign in (-1, 1):
+            got = _fft_kernel_model(x, sign)
+            ref = np.fft.fft(x) if sign < 0 else np.fft.ifft(x) * n
+            assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref))), (n, sign)
