@@ -524,3 +524,32 @@ def test_fft_kernel_index_model_for_every_smooth_length():
             got = _fft_kernel_model(x, sign)
             ref = np.fft.fft(x) if sign < 0 else np.fft.ifft(x) * n
             assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref))), (n, sign)
+
+
+@pytest.mark.parametrize("N,Q", [(8192, 2), (16384, 4), (4 * 3000, 4), (4 * 1537, 4)])
+@pytest.mark.parametrize("shifted", [False, True])
+def test_ring_piece_decomposition(N, Q, shifted):
+    """The decimation in frequency of the piece kernels (ringfft.cu): piece s of a ring of
+    N = Q Lq points computes the outputs Q j + s from a_s[k1] = sum_k2 D[k1 + Lq k2]
+    e^{i pi c (k1 + Lq k2) / N}, c = shifted + 2 s (the ring phase e^{i pi k / N} when
+    phi0 = pi / N, and the piece twiddle), followed by a length-Lq transform; the adjoint
+    gathers b_s[j1] = sum_j2 v[j1 + Lq j2] e^{-2 pi i s (j1 + Lq j2) / N}.  For Q = 2 the
+    k2 = 1 factor is e^{i pi c / 2}, exactly +-1 or +-i."""
+    rng = np.random.default_rng(N + Q)
+    Lq = N // Q
+    D = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    ph = np.exp(1j * np.pi * np.arange(N) / N) if shifted else np.ones(N)
+    ref = np.fft.ifft(D * ph) * N
+    v = rng.standard_normal(N) + 1j * rng.standard_normal(N)
+    W = np.fft.fft(v)
+    k1, k2 = np.arange(Lq)[:, None], np.arange(Q)[None, :]
+    idx = k1 + Lq * k2
+    for s in range(Q):
+        c = (1 if shifted else 0) + 2 * s
+        a = np.sum(D[idx] * np.exp(1j * np.pi * c * (idx % (2 * N)) / N), axis=1)
+        out = np.fft.ifft(a) * Lq
+        assert np.max(np.abs(out - ref[s::Q])) <= 1e-10 * np.max(np.abs(ref))
+        if Q == 2:
+            assert np.isclose(np.exp(1j * np.pi * c * Lq / N), 1j ** (c % 4), atol=1e-15)
+        b = np.sum(v[idx] * np.exp(-2j * np.pi * s * idx / N), axis=1)
+        assert np.max(np.abs(np.fft.fft(b) - W[s::Q])) <= 1e-10 * np.max(np.abs(W))
