@@ -90,6 +90,27 @@ def test_null_pointers_are_rejected(lib):
     assert lib.jhtb_plan_destroy(None) == _lib.JHTB_OK
     assert lib.jhtb_plan_set_watchdog(None, 10**9) == _lib.JHTB_ERR_INVALID
     assert lib.jhtb_plan_inject_fault(None, 1) == _lib.JHTB_ERR_INVALID
+    i64, i32, dbl = ctypes.c_int64(), ctypes.c_int(), ctypes.c_double()
+    ms, counts = (ctypes.c_double * 16)(), (ctypes.c_int64 * 16)()
+    buf = ctypes.c_void_p(16)
+    calls = {
+        "jhtb_plan_bytes": lambda: lib.jhtb_plan_bytes(None, ctypes.byref(i64)),
+        "jhtb_plan_status": lambda: lib.jhtb_plan_status(None, ctypes.byref(i32)),
+        "jhtb_plan_timings": lambda: lib.jhtb_plan_timings(None, ms, counts, 0),
+        "jhtb_plan_set_timing": lambda: lib.jhtb_plan_set_timing(None, 1),
+        "jhtb_plan_set_tuning": lambda: lib.jhtb_plan_set_tuning(None, 0, 0),
+        "jhtb_plan_ring_costs": lambda: lib.jhtb_plan_ring_costs(None, 4, ctypes.byref(i64), 1),
+        "jhtb_plan_set_ring_range": lambda: lib.jhtb_plan_set_ring_range(None, 0, 4),
+        "jhtb_weighted_residual": lambda: lib.jhtb_weighted_residual(None, buf, None, None, buf, 1, None),
+        "jhtb_dot": lambda: lib.jhtb_dot(None, 4, buf, buf, buf, None),
+        "jhtb_axpy": lambda: lib.jhtb_axpy(-1, 1.0, buf, buf, None),
+        "jhtb_probe_fp64_fma": lambda: lib.jhtb_probe_fp64_fma(0, 1, buf, ctypes.byref(dbl), ctypes.byref(dbl), None),
+    }
+    for name, call in calls.items():
+        assert call() == _lib.JHTB_ERR_INVALID, name
+        assert name in _lib.last_error(), name
+    assert lib.jhtb_axpy(4, 1.0, None, buf, None) == _lib.JHTB_ERR_INVALID
+    assert lib.jhtb_axpy(0, 1.0, None, None, None) == _lib.JHTB_OK  # empty: nothing launched
 
 
 @pytest.mark.parametrize("nside", [1, 4, 13, 64])
